@@ -1,0 +1,129 @@
+/*
+ * qsb200.h -- C ABI of the B200 (sm_100a) NEGF solver: QUICHOTTE's self-consistent
+ * loop on the GPU (library libqsb200.so).
+ *
+ * The reference calls these steps from Fortran module procedures; each entry point below
+ * names the reference interface it replaces (file:line, paths relative to the reference
+ * project). A Fortran caller binds them with ISO_C_BINDING; the
+ * argument layout is the one the reference already uses:
+ *   - matrices column-major, complex(dp) = two doubles (re, im);
+ *   - packed SCF vectors in the layout of pack_gf (common/linear_algebra.f90:155-191)
+ *     or pack_nil (src/scf.f90:226-240);
+ *   - state indices 1-based where the reference stores indices (atom_first).
+ * All host pointers are plain host memory; the library owns every device allocation
+ * (made in qs_create, released in qs_destroy).
+ *
+ * Status convention: 0 = success; > 0 = a numerical condition the reference stops on
+ * (e.g. a singular Dyson matrix: 1 + the 0-based energy index); < 0 = CUDA error or
+ * HBM admission failure. The library never aborts the process. qs_last_error() gives
+ * the message of the last failure on a handle.
+ */
+#ifndef QSB200_H
+#define QSB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { QS_PREC_FP64 = 0, QS_PREC_MIXED = 1 };
+
+/* Everything the reference's module globals hold when setup_storage runs
+ * (src/green_functions.f90:43-67, src/scf.f90:38-43, src/parameters.f90). */
+typedef struct qs_problem {
+    int Norb, N_sites, N_atoms, order, n_omega;
+    const double *H;       /* Norb*Norb complex, column-major                      */
+    const double *GammaL;  /* Norb*Norb complex                                    */
+    const double *GammaR;  /* Norb*Norb complex                                    */
+    const double *U_site;  /* Norb (U on the spin-up index of a site)              */
+    const double *omega;   /* n_omega energies                                     */
+    const int *atom_norb;  /* N_atoms                                              */
+    const int *atom_first; /* N_atoms, 1-based                                     */
+    double mu, beta, delta;
+    double alpha_mix, tolf, tolf_order1;
+    int nhist, maxscf, single_history;
+    int precision; /* QS_PREC_FP64 or QS_PREC_MIXED */
+    int device;    /* CUDA device ordinal                                          */
+} qs_problem;
+
+typedef struct qs_scf_step {
+    int step;
+    double fmax, rms;
+    int nh;
+} qs_scf_step;
+
+typedef struct qs_scf_result {
+    int converged;  /* as solve_scf's `converged` (src/scf.f90:142-150)        */
+    int n_iter;
+    double fmax;
+    int aborted;    /* SCF runaway inside broyden_solve                         */
+    int runaway, unphysical, i_worst; /* final_sanity (src/scf.f90:260-275)     */
+    double n_worst, w_worst;
+    int n_resets;   /* Broyden history resets (ill-conditioned Gram matrix)     */
+    qs_scf_step *log; /* caller buffer for the scf_V_<V>.dat lines, or NULL     */
+    int log_cap, n_log;
+    double seconds; /* device time of the solve                                 */
+} qs_scf_result;
+
+typedef struct qs_handle qs_handle;
+
+/* setup_storage + scf_setup_sizes + sigma2_init (src/green_functions.f90:90-190,
+ * src/scf.f90:61-68, src/self_energies.f90:91-106): active subspace, device storage. */
+int qs_create(const qs_problem *p, qs_handle **h);
+/* sigma2_finalize (src/self_energies.f90:108-113) and every other release. */
+void qs_destroy(qs_handle *h);
+const char *qs_last_error(const qs_handle *h);
+
+/* solve_scf(Volt, fresh_start, converged) (src/scf.f90:78-151): converge at Volt, then
+ * the final sweep. fresh_start = 0 continues from the last converged input. */
+int qs_solve_scf(qs_handle *h, double Volt, int fresh_start, qs_scf_result *res);
+
+/* Current(Volt, J_up, J_down) (src/observables.f90:22-39), from the last final sweep. */
+int qs_current(qs_handle *h, double Volt, double *J_up, double *J_down);
+
+/* Arrays the final sweep leaves for the host observables (src/scf.f90:136-139):
+ * G_less_obs (Norb*Norb complex), dosd (Norb*n_omega), trU, trD (n_omega). Any
+ * pointer may be NULL. */
+int qs_get_observables(qs_handle *h, double *G_less_obs, double *dosd, double *trU, double *trD);
+
+/* Sizes: n_vec (src/green_functions.f90:397-405), nA, Nf. */
+int64_t qs_vector_length(const qs_handle *h);
+int qs_active_states(const qs_handle *h);
+int qs_fft_length(const qs_handle *h);
+
+/* ---- finer entry points (one reference routine each; host arrays in and out) ---- */
+
+/* sweep(M_INIT2) + pack_gf (src/scf.f90:116-122) at order 2, or the non-interacting
+ * G^<(t=0) + pack_nil (src/scf.f90:103-110) at order 1: the fresh-start SCF vector. */
+int qs_initial_vector(qs_handle *h, double Volt, double *x);
+
+/* scf_residual2 / scf_residual1 (src/scf.f90:158-224): F = pack(G_out[x]) - x. */
+int qs_residual(qs_handle *h, double Volt, const double *x, double *F, int *abort_flag);
+
+/* unpack_gf + equal_time_lesser + sigma_first_order + sigma2_compute(.true.)
+ * (src/self_energies.f90:45-72,135-219): Sigma2^r, Sigma2^< as (nA,nA,n_omega) complex
+ * column-major, and Sigma1 (Norb*Norb complex); any output may be NULL. */
+int qs_self_energies(qs_handle *h, const double *x, double *SigR2, double *SigL2, double *Sig1);
+
+/* invert_complex (common/linear_algebra.f90:58-88) over a batch: A holds `batch`
+ * N x N complex column-major matrices, replaced by their inverses. info[b] = 0, or k+1
+ * if pivot k of matrix b is zero (the reference's ZGETRF INFO > 0). */
+int qs_invert_batched(int N, int batch, double *A, int *info, int precision);
+
+/* pack_gf / unpack_gf (common/linear_algebra.f90:155-233) for nb x nb x Nw arrays. */
+int qs_pack_gf(int nb, int Nw, const double *Gr, const double *Gl, double *out);
+int qs_unpack_gf(int nb, int Nw, const double *in, double *Gr, double *Gl);
+
+/* broyden_solve (common/broyden_mixing.f90:51-184) with a residual evaluated on the
+ * host: residual(ctx, n, x, F, &abort) gets host arrays. The Broyden state lives on
+ * the device. */
+typedef void (*qs_residual_fn)(void *ctx, int64_t n, const double *x, double *F, int *abort_flag);
+int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t n, double alpha_mix,
+                          int nhist, int maxscf, double tolf, int single_history, int *converged,
+                          int *n_iter, double *fmax, qs_scf_step *log, int log_cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1137 @@
+// oracle.cpp -- CPU oracle for QUICHOTTE's self-consistent NEGF loop.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the checker of the B200 solver: the tests,
+// __graft_entry__.smoke() and the cpu_baseline leg of bench.py call it; nothing in the
+// shipped library links or calls it.
+//
+// It is a line-by-line FP64 restatement of the reference's hot path, with OpenMP where
+// the reference has OpenMP, LAPACK (zgetrf/zgetri/dposv) and BLAS dnrm2 from the
+// OpenBLAS that ships inside the numpy wheel (the reference links OpenBLAS), and a
+// project-written mixed-radix Stockham FFT in place of FFTW3 (same sign and scaling
+// conventions: forward e^{-2 pi i jk/N}, backward e^{+2 pi i jk/N}, both unnormalised).
+//
+// Every routine cites the reference routine it follows (paths relative to the reference
+// project). Parity is pinned by the reference's own 10 physics golden cases
+// (tests/cases/*/reference), compared at its runner's tolerance (tests/run_tests.f90:14).
+//
+// Exported as qso_* with the signatures of include/qsb200.h.
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../include/qsb200.h"
+
+using cplx = std::complex<double>;
+static const cplx IM(0.0, 1.0);
+static const double PI = 3.14159265358979323846;
+static const double HBAR = 1.0;  // common/constants.f90:19
+
+// ------------------------------------------------------------------------------------
+// LAPACK / BLAS from the numpy wheel's OpenBLAS (ILP64, symbol suffix 64_)
+// ------------------------------------------------------------------------------------
+extern "C" {
+void scipy_zgetrf_64_(const int64_t *m, const int64_t *n, cplx *a, const int64_t *lda, int64_t *ipiv, int64_t *info);
+void scipy_zgetri_64_(const int64_t *n, cplx *a, const int64_t *lda, const int64_t *ipiv, cplx *work,
+                      const int64_t *lwork, int64_t *info);
+void scipy_dposv_64_(const char *uplo, const int64_t *n, const int64_t *nrhs, double *a, const int64_t *lda,
+                     double *b, const int64_t *ldb, int64_t *info, size_t uplo_len);
+double scipy_dnrm2_64_(const int64_t *n, const double *x, const int64_t *incx);
+void scipy_openblas_set_num_threads64_(int n);
+}
+
+static double dnrm2(int64_t n, const double *x) {
+    const int64_t one = 1;
+    return scipy_dnrm2_64_(&n, x, &one);
+}
+
+// invert_complex (common/linear_algebra.f90:58-88): zgetrf + zgetri with a workspace
+// query; returns INFO (the reference stops on INFO /= 0).
+static int64_t invert_complex(int N, cplx *A) {
+    int64_t n = N, info = 0, lwork = -1;
+    std::vector<int64_t> ipiv(N);
+    scipy_zgetrf_64_(&n, &n, A, &n, ipiv.data(), &info);
+    if (info != 0) return info;
+    cplx wq;
+    scipy_zgetri_64_(&n, A, &n, ipiv.data(), &wq, &lwork, &info);
+    lwork = (int64_t)wq.real();
+    std::vector<cplx> work(std::max<int64_t>(lwork, 1));
+    scipy_zgetri_64_(&n, A, &n, ipiv.data(), work.data(), &lwork, &info);
+    return info;
+}
+
+// ------------------------------------------------------------------------------------
+// Mixed-radix (2,3,4,5,7,8) Stockham FFT, FFTW conventions (the reference plans
+// dfftw_plan_dft_1d FORWARD/BACKWARD, src/self_energies.f90:102-103).
+// ------------------------------------------------------------------------------------
+struct FFTPlan {
+    int n = 0;
+    std::vector<int> radix;
+    std::vector<cplx> tw;  // tw[k] = exp(-2 pi i k / n)
+    void init(int nn) {
+        n = nn;
+        radix.clear();
+        int m = n;
+        for (int r : {8, 4, 2, 3, 5, 7})
+            while (m % r == 0) { radix.push_back(r); m /= r; }
+        tw.resize(n);
+        for (int k = 0; k < n; k++) {
+            long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)n;
+            tw[k] = cplx((double)cosl(a), (double)sinl(a));
+        }
+    }
+    cplx w(long k, int sign) const {  // exp(sign * 2 pi i k / n)
+        long kk = ((k % n) + n) % n;
+        return sign < 0 ? tw[kk] : std::conj(tw[kk]);
+    }
+    // in-place transform of x (length n); work has length n
+    void exec(cplx *x, cplx *work, int sign) const {
+        cplx *a = x, *b = work;
+        int Ns = 1;
+        cplx v[8], o[8];
+        for (int R : radix) {
+            int nR = n / R;
+            long step = n / R;  // r*k/(Ns*R) in units of 1/n: r*k*(n/(Ns*R))
+            for (int j = 0; j < nR; j++) {
+                int k = j % Ns;
+                long tws = (long)k * (n / (Ns * R));
+                for (int r = 0; r < R; r++) v[r] = a[j + r * nR] * (r ? w(r * tws, sign) : cplx(1.0));
+                for (int q = 0; q < R; q++) {
+                    cplx s = v[0];
+                    for (int r = 1; r < R; r++) s += v[r] * w((long)r * q * (n / R), sign);
+                    o[q] = s;
+                }
+                int idxD = (j / Ns) * Ns * R + k;
+                for (int r = 0; r < R; r++) b[idxD + r * Ns] = o[r];
+            }
+            (void)step;
+            std::swap(a, b);
+            Ns *= R;
+        }
+        if (a != x) std::memcpy(x, a, sizeof(cplx) * n);
+    }
+};
+
+// ------------------------------------------------------------------------------------
+// Solver state: the module globals of GreenFunctions, SelfEnergies and SCF
+// ------------------------------------------------------------------------------------
+struct qso_state {
+    // problem
+    int Norb = 0, N_sites = 0, N_atoms = 0, order = 0, n = 0;
+    std::vector<cplx> H, GammaL, GammaR;
+    std::vector<double> U_site, omega;
+    std::vector<int> atom_norb, atom_first;
+    double mu = 0, beta = 0, delta = 0;
+    double alpha_mix = 0.5, tolf = 1e-6, tolf_order1 = 1e-8;
+    int nhist = 16, maxscf = 300;
+    bool single_history = true;
+    // setup_storage
+    int nA = 0, nS = 0, nCL = 0, nAs = 0, n_int_sites = 0;
+    std::vector<int> act, pos, sup, cl, asite;  // 1-based values, as in the reference
+    std::vector<char> site_int, site_act;
+    std::vector<cplx> Hemb, Sig1, GamL_s, GamR_s, GamL_cl, G_less_t0, G_less_obs;
+    std::vector<cplx> Gr_in, GL_in;  // (nA, nA, n)
+    std::vector<cplx> gRd, gLd;      // (nA, n)
+    std::vector<cplx> onsL;          // (4 N_sites, n)
+    std::vector<double> dosd;        // (Norb, n)
+    std::vector<cplx> atomL;         // (atom_off(N_atoms+1), n)
+    std::vector<int> atom_off;
+    bool has_atomL = false;
+    std::vector<double> trU, trD;
+    int n_full = 0, n_strict_upper = 0, n_upper = 0, nblk = 0;
+    int64_t n_vec = 0;
+    // SelfEnergies
+    int Nf = 0;
+    FFTPlan plan;
+    std::vector<cplx> Fr, FL, SigR2, SigL2;
+    bool sigma2_ready = false;
+    // SCF
+    bool use_sigma = false;
+    double V_scf = 0;
+    int scf_iter = 0;
+    std::vector<double> x_keep;  // converged input of the last voltage (continuation)
+    bool have_x = false;
+    std::string err;
+    int64_t singular = 0;
+
+    cplx &H_(int i, int j) { return H[(i - 1) + (size_t)(j - 1) * Norb]; }
+};
+
+static inline cplx &at2(std::vector<cplx> &A, int ld, int i, int j) { return A[(i - 1) + (size_t)(j - 1) * ld]; }
+static inline cplx &at3(std::vector<cplx> &A, int ld, int i, int j, int k) {
+    return A[(i - 1) + (size_t)(j - 1) * ld + (size_t)(k - 1) * ld * ld];
+}
+
+// fermi (src/green_functions.f90:74-84)
+static double fermi(const qso_state &s, double w, double V) {
+    double arg = (w - s.mu + V / HBAR) * s.beta;
+    return 1.0 / (std::exp(std::min(HBAR * arg, 700.0)) + 1.0);
+}
+
+// setup_storage (src/green_functions.f90:90-190) + scf_setup_sizes (src/scf.f90:61-68)
+static void setup_storage(qso_state &s) {
+    const int No = s.Norb;
+    s.site_int.assign(s.N_sites + 1, 0);
+    s.site_act.assign(s.N_sites + 1, 0);
+    s.pos.assign(No + 1, 0);
+    std::vector<char> conL(No + 1, 0), conR(No + 1, 0);
+    for (int st = 1; st <= s.N_sites; st++) s.site_int[st] = (s.order >= 1 && s.U_site[2 * st - 2] != 0.0);
+    s.n_int_sites = 0;
+    for (int st = 1; st <= s.N_sites; st++) s.n_int_sites += s.site_int[st];
+    for (int st = 1; st <= s.N_sites; st++) s.site_act[st] = s.site_int[st];
+    for (int i = 1; i <= No; i++) {
+        bool l = false, r = false;
+        for (int j = 1; j <= No; j++) {
+            l = l || at2(s.GammaL, No, i, j) != 0.0 || at2(s.GammaL, No, j, i) != 0.0;
+            r = r || at2(s.GammaR, No, i, j) != 0.0 || at2(s.GammaR, No, j, i) != 0.0;
+        }
+        conL[i] = l;
+        conR[i] = r;
+        if (l || r) s.site_act[(i + 1) / 2] = 1;
+    }
+    s.act.clear();
+    for (int i = 1; i <= No; i++)
+        if (s.site_act[(i + 1) / 2]) { s.act.push_back(i); s.pos[i] = (int)s.act.size(); }
+    s.nA = (int)s.act.size();
+    s.asite.clear();
+    for (int st = 1; st <= s.N_sites; st++)
+        if (s.site_act[st]) s.asite.push_back(st);
+    s.nAs = (int)s.asite.size();
+    s.cl.clear();
+    for (int i = 1; i <= No; i++)
+        if (conL[i]) s.cl.push_back(i);
+    s.nCL = (int)s.cl.size();
+    s.sup.clear();
+    if (s.order == 2) s.sup = s.act;
+    else
+        for (int i = 1; i <= No; i++)
+            if (conL[i] || conR[i]) s.sup.push_back(i);
+    s.nS = (int)s.sup.size();
+    s.GamL_s.assign((size_t)s.nS * s.nS, 0.0);
+    s.GamR_s.assign((size_t)s.nS * s.nS, 0.0);
+    s.GamL_cl.assign((size_t)s.nCL * s.nCL, 0.0);
+    for (int b = 1; b <= s.nS; b++)
+        for (int a = 1; a <= s.nS; a++) {
+            at2(s.GamL_s, s.nS, a, b) = at2(s.GammaL, No, s.sup[a - 1], s.sup[b - 1]);
+            at2(s.GamR_s, s.nS, a, b) = at2(s.GammaR, No, s.sup[a - 1], s.sup[b - 1]);
+        }
+    for (int b = 1; b <= s.nCL; b++)
+        for (int a = 1; a <= s.nCL; a++) at2(s.GamL_cl, s.nCL, a, b) = at2(s.GammaL, No, s.cl[a - 1], s.cl[b - 1]);
+    s.Hemb.assign((size_t)No * No, 0.0);
+    s.Sig1.assign((size_t)No * No, 0.0);
+    s.G_less_t0.assign((size_t)No * No, 0.0);
+    s.G_less_obs.assign((size_t)No * No, 0.0);
+    s.onsL.assign((size_t)4 * s.N_sites * s.n, 0.0);
+    s.dosd.assign((size_t)No * s.n, 0.0);
+    s.trU.assign(s.n, 0.0);
+    s.trD.assign(s.n, 0.0);
+    int mx = 0;
+    for (int v : s.atom_norb) mx = std::max(mx, v);
+    s.has_atomL = mx > 1;
+    if (s.has_atomL) {
+        s.atom_off.assign(s.N_atoms + 1, 0);
+        for (int i = 1; i <= s.N_atoms; i++) s.atom_off[i] = s.atom_off[i - 1] + (2 * s.atom_norb[i - 1]) * (2 * s.atom_norb[i - 1]);
+        s.atomL.assign((size_t)s.atom_off[s.N_atoms] * s.n, 0.0);
+    }
+    if (s.order >= 1) {
+        s.gRd.assign((size_t)s.nA * s.n, 0.0);
+        s.gLd.assign((size_t)s.nA * s.n, 0.0);
+    }
+    s.n_vec = 0;
+    if (s.order == 1) s.n_vec = 8 * s.n_int_sites;
+    else if (s.order == 2) {
+        int64_t nfull = (int64_t)s.nA * s.nA, nsu = (nfull - s.nA) / 2;
+        s.n_vec = (2 * nfull + nsu + nsu + s.nA) * s.n;
+        s.Gr_in.assign((size_t)nfull * s.n, 0.0);
+        s.GL_in.assign((size_t)nfull * s.n, 0.0);
+    }
+    s.n_full = s.nA * s.nA;
+    s.n_strict_upper = (s.n_full - s.nA) / 2;
+    s.n_upper = s.n_strict_upper + s.nA;
+    s.nblk = 2 * s.n_full + s.n_strict_upper + s.n_upper;
+}
+
+// equal_time_lesser (src/green_functions.f90:192-213)
+static void equal_time_lesser(qso_state &s) {
+    double pp = s.delta / (2.0 * PI);
+    std::fill(s.G_less_t0.begin(), s.G_less_t0.end(), 0.0);
+    for (int is = 1; is <= s.nAs; is++)
+        for (int a = 2 * s.asite[is - 1] - 1; a <= 2 * s.asite[is - 1]; a++)
+            for (int b = 2 * s.asite[is - 1] - 1; b <= 2 * s.asite[is - 1]; b++) {
+                cplx acc = 0.0;
+                for (int k1 = 1; k1 <= s.n; k1++) acc += at3(s.GL_in, s.nA, s.pos[a], s.pos[b], k1);
+                at2(s.G_less_t0, s.Norb, a, b) = acc * pp;
+            }
+}
+
+// gather_onsite (src/green_functions.f90:215-238)
+static void gather_onsite(qso_state &s, const std::vector<char> &mask, std::vector<cplx> &G) {
+    double pp = s.delta / (2.0 * PI);
+    for (int st = 1; st <= s.N_sites; st++) {
+        if (!mask[st]) continue;
+        for (int b = 1; b <= 2; b++)
+            for (int a = 1; a <= 2; a++) {
+                int k = 4 * (st - 1) + 2 * (b - 1) + a;
+                cplx acc = 0.0;
+                for (int iw = 1; iw <= s.n; iw++) acc += s.onsL[(k - 1) + (size_t)(iw - 1) * 4 * s.N_sites];
+                at2(G, s.Norb, 2 * st - 2 + a, 2 * st - 2 + b) = acc * pp;
+            }
+    }
+}
+
+// gather_atoms (src/green_functions.f90:240-257)
+static void gather_atoms(qso_state &s, std::vector<cplx> &G) {
+    if (!s.has_atomL) return;
+    double pp = s.delta / (2.0 * PI);
+    size_t ld = s.atom_off[s.N_atoms];
+    for (int at = 1; at <= s.N_atoms; at++) {
+        int m = 2 * s.atom_norb[at - 1], lo = 2 * s.atom_first[at - 1] - 2;
+        for (int b = 1; b <= m; b++)
+            for (int a = 1; a <= m; a++) {
+                cplx acc = 0.0;
+                size_t row = s.atom_off[at - 1] + (b - 1) * m + a - 1;
+                for (int iw = 0; iw < s.n; iw++) acc += s.atomL[row + iw * ld];
+                at2(G, s.Norb, lo + a, lo + b) = acc * pp;
+            }
+    }
+}
+
+// sigma_first_order (src/self_energies.f90:45-72)
+static void sigma_first_order(qso_state &s) {
+    std::fill(s.Sig1.begin(), s.Sig1.end(), 0.0);
+    for (int i = 1; i <= s.Norb; i += 2) {
+        cplx hartree = at2(s.G_less_t0, s.Norb, i, i) + at2(s.G_less_t0, s.Norb, i + 1, i + 1);
+        for (int a = 0; a <= 1; a++)
+            for (int b = 0; b <= 1; b++) {
+                if (a == b)
+                    at2(s.Sig1, s.Norb, i + a, i + b) = IM * HBAR * s.U_site[i - 1] * (at2(s.G_less_t0, s.Norb, i + a, i + b) - hartree);
+                else
+                    at2(s.Sig1, s.Norb, i + a, i + b) = IM * HBAR * s.U_site[i - 1] * at2(s.G_less_t0, s.Norb, i + a, i + b);
+            }
+    }
+}
+
+// good_fft_size (src/self_energies.f90:75-89)
+static int good_fft_size(int nmin) {
+    int n = nmin;
+    for (;;) {
+        int m = n;
+        while (m % 2 == 0) m /= 2;
+        while (m % 3 == 0) m /= 3;
+        while (m % 5 == 0) m /= 5;
+        while (m % 7 == 0) m /= 7;
+        if (m == 1) return n;
+        n++;
+    }
+}
+
+// sigma2_init (src/self_energies.f90:91-106)
+static void sigma2_init(qso_state &s) {
+    s.Nf = good_fft_size(2 * s.n - 1);
+    s.Fr.assign((size_t)s.Nf * s.nA * s.nA, 0.0);
+    s.FL.assign((size_t)s.Nf * s.nA * s.nA, 0.0);
+    s.SigR2.assign((size_t)s.nA * s.nA * s.n, 0.0);
+    s.SigL2.assign((size_t)s.nA * s.nA * s.n, 0.0);
+    s.plan.init(s.Nf);
+    s.sigma2_ready = true;
+}
+
+// adj2 (src/self_energies.f90:222-228)
+struct M2 { cplx a[2][2]; };
+static inline M2 adj2(const M2 &M) {
+    M2 A;
+    A.a[0][0] = M.a[1][1];
+    A.a[0][1] = -M.a[0][1];
+    A.a[1][0] = -M.a[1][0];
+    A.a[1][1] = M.a[0][0];
+    return A;
+}
+static inline M2 mm(const M2 &X, const M2 &Y) {
+    M2 Z;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) Z.a[i][j] = X.a[i][0] * Y.a[0][j] + X.a[i][1] * Y.a[1][j];
+    return Z;
+}
+static inline M2 dag(const M2 &X) {
+    M2 Z;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) Z.a[i][j] = std::conj(X.a[j][i]);
+    return Z;
+}
+
+// sigma2_compute (src/self_energies.f90:135-219)
+static void sigma2_compute(qso_state &s, bool do_lesser) {
+    const int nA = s.nA, Nf = s.Nf, n = s.n;
+    double pp = s.delta / (2.0 * PI);
+    // 1. forward FFT of every active element of G^r and G^< (load_fft, lines 116-130)
+#pragma omp parallel
+    {
+        std::vector<cplx> work(Nf);
+#pragma omp for collapse(2) schedule(static)
+        for (int jj = 1; jj <= nA; jj++)
+            for (int ii = 1; ii <= nA; ii++) {
+                cplx *dr = &s.Fr[(size_t)Nf * ((ii - 1) + (size_t)(jj - 1) * nA)];
+                cplx *dl = &s.FL[(size_t)Nf * ((ii - 1) + (size_t)(jj - 1) * nA)];
+                for (int iw = 1; iw <= n; iw++) {
+                    dr[iw - 1] = at3(s.Gr_in, nA, ii, jj, iw);
+                    dl[iw - 1] = at3(s.GL_in, nA, ii, jj, iw);
+                }
+                for (int k = n; k < Nf; k++) dr[k] = dl[k] = 0.0;
+                s.plan.exec(dr, work.data(), -1);
+                s.plan.exec(dl, work.data(), -1);
+            }
+    }
+    auto Fr = [&](int l, int i, int j) { return s.Fr[(size_t)(l - 1) + (size_t)Nf * ((i - 1) + (size_t)(j - 1) * nA)]; };
+    auto FL = [&](int l, int i, int j) { return s.FL[(size_t)(l - 1) + (size_t)Nf * ((i - 1) + (size_t)(j - 1) * nA)]; };
+    // 2. per pair of active sites: 2x2 algebra at every l, then inverse FFT
+#pragma omp parallel
+    {
+        std::vector<cplx> bufR((size_t)Nf * 4), bufL((size_t)Nf * 4), work(Nf);
+#pragma omp for collapse(2) schedule(dynamic)
+        for (int ja = 1; ja <= s.nAs; ja++)
+            for (int ia = 1; ia <= s.nAs; ia++) {
+                int io = s.pos[2 * s.asite[ia - 1] - 1], jo = s.pos[2 * s.asite[ja - 1] - 1];
+                double Uprod = s.U_site[s.act[io - 1] - 1] * s.U_site[s.act[jo - 1] - 1];
+                if (Uprod == 0.0) {
+                    for (int iw = 1; iw <= n; iw++)
+                        for (int a = 0; a < 2; a++)
+                            for (int b = 0; b < 2; b++) {
+                                at3(s.SigR2, nA, io + a, jo + b, iw) = 0.0;
+                                at3(s.SigL2, nA, io + a, jo + b, iw) = 0.0;
+                            }
+                    continue;
+                }
+                for (int l = 1; l <= Nf; l++) {
+                    int lm = (Nf - (l - 1)) % Nf + 1;
+                    M2 r_ij, L_ij, r_ji, L_ji;
+                    for (int a = 0; a < 2; a++)
+                        for (int b = 0; b < 2; b++) {
+                            r_ij.a[a][b] = Fr(l, io + a, jo + b);
+                            L_ij.a[a][b] = FL(l, io + a, jo + b);
+                            r_ji.a[a][b] = Fr(lm, jo + a, io + b);
+                            L_ji.a[a][b] = FL(lm, jo + a, io + b);
+                        }
+                    M2 a_ij = dag(r_ji), a_ji = dag(r_ij), G_ij, G_ji;
+                    for (int a = 0; a < 2; a++)
+                        for (int b = 0; b < 2; b++) {
+                            G_ij.a[a][b] = L_ij.a[a][b] + r_ij.a[a][b] - a_ij.a[a][b];
+                            G_ji.a[a][b] = L_ji.a[a][b] + r_ji.a[a][b] - a_ji.a[a][b];
+                        }
+                    M2 chi1 = mm(L_ji, G_ij);
+                    M2 t1 = mm(L_ji, r_ij), t2 = mm(a_ji, L_ij), chi2;
+                    for (int a = 0; a < 2; a++)
+                        for (int b = 0; b < 2; b++) chi2.a[a][b] = t1.a[a][b] + t2.a[a][b];
+                    M2 u1 = mm(r_ij, adj2(chi1)), u2 = mm(L_ij, adj2(chi2));
+                    for (int a = 0; a < 2; a++)
+                        for (int b = 0; b < 2; b++) bufR[(size_t)(l - 1) + (size_t)Nf * (a + 2 * b)] = u1.a[a][b] + u2.a[a][b];
+                    if (do_lesser) {
+                        M2 chiL = mm(G_ji, L_ij);
+                        M2 sL = mm(L_ij, adj2(chiL));
+                        for (int a = 0; a < 2; a++)
+                            for (int b = 0; b < 2; b++) bufL[(size_t)(l - 1) + (size_t)Nf * (a + 2 * b)] = sL.a[a][b];
+                    }
+                }
+                cplx c = Uprod * HBAR * HBAR * pp * pp / (double)Nf;
+                for (int sp1 = 1; sp1 <= 2; sp1++)
+                    for (int sp = 1; sp <= 2; sp++) {
+                        cplx *bR = &bufR[(size_t)Nf * ((sp - 1) + 2 * (sp1 - 1))];
+                        s.plan.exec(bR, work.data(), +1);
+                        for (int iw = 1; iw <= n; iw++) at3(s.SigR2, nA, io + sp - 1, jo + sp1 - 1, iw) = c * bR[iw - 1];
+                        if (do_lesser) {
+                            cplx *bL = &bufL[(size_t)Nf * ((sp - 1) + 2 * (sp1 - 1))];
+                            s.plan.exec(bL, work.data(), +1);
+                            for (int iw = 1; iw <= n; iw++) at3(s.SigL2, nA, io + sp - 1, jo + sp1 - 1, iw) = c * bL[iw - 1];
+                        }
+                    }
+            }
+    }
+}
+
+// pack_gf (common/linear_algebra.f90:155-191), one energy block or Nw of them
+static void pack_gf(const cplx *In1, const cplx *In2, double *out, int n_full, int n_strict_upper, int nb, int Nw) {
+    int nblock = 2 * n_full + n_strict_upper + (n_strict_upper + nb);
+    for (int iw = 1; iw <= Nw; iw++) {
+        size_t off = (size_t)(iw - 1) * nblock;
+        const cplx *A = In1 + (size_t)(iw - 1) * nb * nb, *B = In2 + (size_t)(iw - 1) * nb * nb;
+        int n = 0;
+        for (int i = 1; i <= nb; i++)
+            for (int j = 1; j <= nb; j++) {
+                n++;
+                out[off + n - 1] = A[(i - 1) + (size_t)(j - 1) * nb].real();
+                out[off + n + n_full - 1] = A[(i - 1) + (size_t)(j - 1) * nb].imag();
+            }
+        n = 2 * n_full + n_strict_upper;
+        int n1 = 2 * n_full;
+        for (int i = 1; i <= nb; i++)
+            for (int j = i; j <= nb; j++) {
+                n++;
+                if (i != j) { n1++; out[off + n1 - 1] = B[(i - 1) + (size_t)(j - 1) * nb].real(); }
+                out[off + n - 1] = B[(i - 1) + (size_t)(j - 1) * nb].imag();
+            }
+    }
+}
+
+// unpack_gf (common/linear_algebra.f90:193-233)
+static void unpack_gf(cplx *O1, cplx *O2, const double *in, int n_full, int n_strict_upper, int nb, int Nw) {
+    int nblock = 2 * n_full + n_strict_upper + (n_strict_upper + nb);
+    for (int iw = 1; iw <= Nw; iw++) {
+        size_t off = (size_t)(iw - 1) * nblock;
+        cplx *A = O1 + (size_t)(iw - 1) * nb * nb, *B = O2 + (size_t)(iw - 1) * nb * nb;
+        int n = 0;
+        for (int i = 1; i <= nb; i++)
+            for (int j = 1; j <= nb; j++) {
+                n++;
+                A[(i - 1) + (size_t)(j - 1) * nb] = cplx(in[off + n - 1], in[off + n + n_full - 1]);
+            }
+        n = 2 * n_full + n_strict_upper;
+        int n1 = 2 * n_full;
+        for (int i = 1; i <= nb; i++)
+            for (int j = i; j <= nb; j++) {
+                n++;
+                double re = 0.0;
+                if (i != j) { n1++; re = in[off + n1 - 1]; }
+                B[(i - 1) + (size_t)(j - 1) * nb] = cplx(re, in[off + n - 1]);
+                B[(j - 1) + (size_t)(i - 1) * nb] = -std::conj(B[(i - 1) + (size_t)(j - 1) * nb]);
+            }
+    }
+}
+
+enum { M_INIT2 = 1, M_SCF2 = 2, M_SCF1 = 3, M_FINAL = 4 };
+
+// G_at_energy (src/scf.f90:305-415)
+static void G_at_energy(qso_state &s, int iw, double Volt, int mode, double *F) {
+    const int No = s.Norb, nA = s.nA, nS = s.nS;
+    double w = s.omega[iw - 1];
+    std::vector<cplx> w1(s.Hemb);
+    if (s.use_sigma) {
+        for (int b = 1; b <= nA; b++)
+            for (int a = 1; a <= nA; a++) {
+                cplx sg = at2(s.Sig1, No, s.act[a - 1], s.act[b - 1]);
+                if (s.order == 2) sg += at3(s.SigR2, nA, a, b, iw);
+                at2(w1, No, s.act[a - 1], s.act[b - 1]) -= sg;
+            }
+    }
+    for (int i = 1; i <= No; i++) at2(w1, No, i, i) += HBAR * w;
+    int64_t info = invert_complex(No, w1.data());
+    if (info != 0) {
+#pragma omp critical
+        s.singular = iw;
+    }
+    auto W = [&](int i, int j) { return w1[(i - 1) + (size_t)(j - 1) * No]; };
+
+    double fL = fermi(s, w, Volt), fR = fermi(s, w, 0.0);
+    std::vector<cplx> SL((size_t)nS * nS);
+    for (size_t k = 0; k < SL.size(); k++) SL[k] = IM * (fL * s.GamL_s[k] + fR * s.GamR_s[k]) / HBAR;
+    if (s.use_sigma && s.order == 2)
+        for (int b = 1; b <= nS; b++)
+            for (int a = 1; a <= nS; a++) at2(SL, nS, a, b) += at3(s.SigL2, nA, a, b, iw);
+
+    if (mode == M_INIT2 || mode == M_SCF2) {
+        // sup = act: grA = w1(act,act); T = grA SL; glA = T grA^dagger
+        std::vector<cplx> grA((size_t)nA * nA), T((size_t)nA * nA, 0.0), glA((size_t)nA * nA, 0.0);
+        for (int b = 1; b <= nA; b++)
+            for (int a = 1; a <= nA; a++) grA[(a - 1) + (size_t)(b - 1) * nA] = W(s.act[a - 1], s.act[b - 1]);
+        for (int j = 0; j < nA; j++)
+            for (int k = 0; k < nA; k++) {
+                cplx b = SL[k + (size_t)j * nA];
+                for (int i = 0; i < nA; i++) T[i + (size_t)j * nA] += grA[i + (size_t)k * nA] * b;
+            }
+        for (int j = 0; j < nA; j++)
+            for (int k = 0; k < nA; k++) {
+                cplx b = std::conj(grA[j + (size_t)k * nA]);
+                for (int i = 0; i < nA; i++) glA[i + (size_t)j * nA] += T[i + (size_t)k * nA] * b;
+            }
+        if (mode == M_INIT2) {
+            std::copy(grA.begin(), grA.end(), s.Gr_in.begin() + (size_t)(iw - 1) * nA * nA);
+            std::copy(glA.begin(), glA.end(), s.GL_in.begin() + (size_t)(iw - 1) * nA * nA);
+        } else {
+            size_t off = (size_t)(iw - 1) * s.nblk;
+            pack_gf(grA.data(), glA.data(), F + off, s.n_full, s.n_strict_upper, nA, 1);
+            for (int k = 1; k <= nA; k++) {
+                s.gRd[(k - 1) + (size_t)(iw - 1) * nA] = grA[(k - 1) + (size_t)(k - 1) * nA];
+                s.gLd[(k - 1) + (size_t)(iw - 1) * nA] = glA[(k - 1) + (size_t)(k - 1) * nA];
+            }
+        }
+    } else if (mode == M_SCF1) {
+        // T = w1(act, sup) SL
+        std::vector<cplx> T((size_t)nA * nS, 0.0);
+        for (int j = 1; j <= nS; j++)
+            for (int k = 1; k <= nS; k++) {
+                cplx b = at2(SL, nS, k, j);
+                for (int i = 1; i <= nA; i++) T[(i - 1) + (size_t)(j - 1) * nA] += W(s.act[i - 1], s.sup[k - 1]) * b;
+            }
+        for (int k = 1; k <= nA; k++) {
+            s.gRd[(k - 1) + (size_t)(iw - 1) * nA] = W(s.act[k - 1], s.act[k - 1]);
+            cplx acc = 0.0;
+            for (int q = 1; q <= nS; q++) acc += T[(k - 1) + (size_t)(q - 1) * nA] * std::conj(W(s.act[k - 1], s.sup[q - 1]));
+            s.gLd[(k - 1) + (size_t)(iw - 1) * nA] = acc;
+        }
+        for (int st = 1; st <= s.N_sites; st++) {
+            if (!s.site_int[st]) continue;
+            int lo = 2 * st - 1, p1 = s.pos[lo];
+            for (int b = 0; b < 2; b++)
+                for (int a = 0; a < 2; a++) {
+                    cplx acc = 0.0;
+                    for (int q = 1; q <= nS; q++)
+                        acc += T[(p1 + a - 1) + (size_t)(q - 1) * nA] * std::conj(W(lo + b, s.sup[q - 1]));
+                    s.onsL[(size_t)(4 * (st - 1) + a + 2 * b) + (size_t)(iw - 1) * 4 * s.N_sites] = acc;
+                }
+        }
+    } else {  // M_FINAL
+        std::vector<cplx> T((size_t)No * nS, 0.0);
+        for (int j = 1; j <= nS; j++)
+            for (int k = 1; k <= nS; k++) {
+                cplx b = at2(SL, nS, k, j);
+                if (b == 0.0) continue;
+                for (int i = 1; i <= No; i++) T[(i - 1) + (size_t)(j - 1) * No] += W(i, s.sup[k - 1]) * b;
+            }
+        for (int i = 1; i <= No; i++) s.dosd[(i - 1) + (size_t)(iw - 1) * No] = W(i, i).imag();
+        auto blk = [&](int ra, int rb) {  // sum_q T(ra,q) conj(w1(rb, sup(q)))
+            cplx acc = 0.0;
+            for (int q = 1; q <= nS; q++) acc += T[(ra - 1) + (size_t)(q - 1) * No] * std::conj(W(rb, s.sup[q - 1]));
+            return acc;
+        };
+        for (int st = 1; st <= s.N_sites; st++) {
+            int lo = 2 * st - 1;
+            for (int b = 0; b < 2; b++)
+                for (int a = 0; a < 2; a++)
+                    s.onsL[(size_t)(4 * (st - 1) + a + 2 * b) + (size_t)(iw - 1) * 4 * s.N_sites] = blk(lo + a, lo + b);
+        }
+        if (s.has_atomL) {
+            size_t ld = s.atom_off[s.N_atoms];
+            for (int at = 1; at <= s.N_atoms; at++) {
+                int lo = 2 * s.atom_first[at - 1] - 1, m = 2 * s.atom_norb[at - 1];
+                for (int b = 0; b < m; b++)
+                    for (int a = 0; a < m; a++)
+                        s.atomL[(size_t)(s.atom_off[at - 1] + a + b * m) + (size_t)(iw - 1) * ld] = blk(lo + a, lo + b);
+            }
+        }
+        // current integrand through the left lead (src/scf.f90:390-409)
+        const int nCL = s.nCL;
+        std::vector<cplx> GLc((size_t)nCL * nCL), X((size_t)nCL * nCL);
+        for (int a = 1; a <= nCL; a++)
+            for (int k = 1; k <= nCL; k++) GLc[(k - 1) + (size_t)(a - 1) * nCL] = blk(s.cl[k - 1], s.cl[a - 1]);
+        for (int a = 1; a <= nCL; a++)
+            for (int k = 1; k <= nCL; k++) {
+                cplx g = GLc[(k - 1) + (size_t)(a - 1) * nCL];
+                X[(k - 1) + (size_t)(a - 1) * nCL] =
+                    (fL - 1.0) * g - fL * (g + W(s.cl[k - 1], s.cl[a - 1]) - std::conj(W(s.cl[a - 1], s.cl[k - 1])));
+            }
+        cplx tu = 0.0, td = 0.0;
+        for (int a = 1; a <= nCL; a++) {
+            cplx mc = 0.0;  // Mc(a,a) = i sum_k GamL_cl(a,k) X(k,a)
+            for (int k = 1; k <= nCL; k++) mc += at2(s.GamL_cl, nCL, a, k) * X[(k - 1) + (size_t)(a - 1) * nCL];
+            mc *= IM;
+            if (s.cl[a - 1] % 2 == 1) tu += mc;
+            else td += mc;
+        }
+        s.trU[iw - 1] = tu.real() / (2.0 * PI);
+        s.trD[iw - 1] = td.real() / (2.0 * PI);
+    }
+}
+
+// sweep (src/scf.f90:280-290)
+static void sweep(qso_state &s, int mode, double *F) {
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int iw = 1; iw <= s.n; iw++) G_at_energy(s, iw, s.V_scf, mode, F);
+}
+
+// check_diag_sanity (common/scf_checks.f90:59-91)
+static void check_diag_sanity(const cplx *Grd, const cplx *GLd, int nb, int nw, double delta, bool &runaway,
+                              bool &unphysical, int &i_worst, double &n_worst, double &w_worst, const int *state_index) {
+    runaway = false;
+    unphysical = false;
+    i_worst = 1;
+    n_worst = 0.5;
+    w_worst = 1.0;
+    for (int i = 1; i <= nb; i++) {
+        int lab = state_index ? state_index[i - 1] : i;
+        cplx sl = 0.0;
+        double si = 0.0;
+        for (int w = 0; w < nw; w++) {
+            sl += GLd[(i - 1) + (size_t)w * nb];
+            si += Grd[(i - 1) + (size_t)w * nb].imag();
+        }
+        double nocc = (-IM * HBAR * (delta / (2.0 * PI)) * sl).real();
+        double wsum = -HBAR * (delta / PI) * si;
+        if (!std::isfinite(nocc) || !std::isfinite(wsum)) {
+            runaway = true;
+            unphysical = true;
+            i_worst = lab;
+            n_worst = nocc;
+            w_worst = wsum;
+            return;
+        }
+        if (nocc < -1.0 || nocc > 2.0) runaway = true;
+        if (nocc < -0.05 || nocc > 1.05 || wsum < 0.5) unphysical = true;
+        if (std::fabs(nocc - 0.5) > std::fabs(n_worst - 0.5) || (wsum < w_worst && std::fabs(n_worst - 0.5) <= 0.55)) {
+            i_worst = lab;
+            n_worst = nocc;
+            w_worst = wsum;
+        }
+    }
+    if (runaway) unphysical = true;
+}
+
+// pack_nil / unpack_nil (src/scf.f90:226-255)
+static void pack_nil(qso_state &s, const std::vector<cplx> &G, double *x) {
+    int k = 0;
+    for (int st = 1; st <= s.N_sites; st++) {
+        if (!s.site_int[st]) continue;
+        for (int b = 2 * st - 1; b <= 2 * st; b++)
+            for (int a = 2 * st - 1; a <= 2 * st; a++) {
+                cplx g = G[(a - 1) + (size_t)(b - 1) * s.Norb];
+                x[k] = g.real();
+                x[k + 1] = g.imag();
+                k += 2;
+            }
+    }
+}
+static void unpack_nil(qso_state &s, const double *x, std::vector<cplx> &G) {
+    std::fill(G.begin(), G.end(), 0.0);
+    int k = 0;
+    for (int st = 1; st <= s.N_sites; st++) {
+        if (!s.site_int[st]) continue;
+        for (int b = 2 * st - 1; b <= 2 * st; b++)
+            for (int a = 2 * st - 1; a <= 2 * st; a++) {
+                G[(a - 1) + (size_t)(b - 1) * s.Norb] = cplx(x[k], x[k + 1]);
+                k += 2;
+            }
+    }
+}
+
+// scf_residual2 (src/scf.f90:158-188)
+static void scf_residual2(qso_state &s, int64_t n, const double *x, double *F, bool &abort) {
+    s.scf_iter++;
+    unpack_gf(s.Gr_in.data(), s.GL_in.data(), x, s.n_full, s.n_strict_upper, s.nA, s.n);
+    equal_time_lesser(s);
+    sigma_first_order(s);
+    sigma2_compute(s, true);
+    s.use_sigma = true;
+    sweep(s, M_SCF2, F);
+    bool unphys;
+    int iw;
+    double nw, ww;
+    check_diag_sanity(s.gRd.data(), s.gLd.data(), s.nA, s.n, s.delta, abort, unphys, iw, nw, ww, s.act.data());
+    if (abort) {
+        std::fill(F, F + n, 0.0);
+        return;
+    }
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; i++) F[i] -= x[i];
+}
+
+// scf_residual1 (src/scf.f90:194-224)
+static void scf_residual1(qso_state &s, int64_t n, const double *x, double *F, bool &abort) {
+    s.scf_iter++;
+    unpack_nil(s, x, s.G_less_t0);
+    sigma_first_order(s);
+    s.use_sigma = true;
+    sweep(s, M_SCF1, F);
+    bool unphys;
+    int iw;
+    double nw, ww;
+    check_diag_sanity(s.gRd.data(), s.gLd.data(), s.nA, s.n, s.delta, abort, unphys, iw, nw, ww, s.act.data());
+    if (abort) {
+        std::fill(F, F + n, 0.0);
+        return;
+    }
+    std::vector<cplx> Gout((size_t)s.Norb * s.Norb, 0.0);
+    gather_onsite(s, s.site_int, Gout);
+    pack_nil(s, Gout, F);
+    for (int64_t i = 0; i < n; i++) F[i] -= x[i];
+}
+
+// broyden_solve (common/broyden_mixing.f90:51-184), with its dot_ss / dot_sd (186-215)
+template <class Residual>
+static void broyden_solve(Residual residual, double *x, int64_t n, double alpha_mix, int nhist, int maxscf, double tolf,
+                          bool sp, bool &converged, int &n_iter, double &fmax, std::vector<qs_scf_step> &log,
+                          int &n_resets) {
+    const double w0 = 0.01;
+    int lda = std::max(nhist, 1);
+    std::vector<double> F(n), Fold(n), xold(n), a((size_t)lda * lda), cvec(lda), gram((size_t)lda * lda);
+    std::vector<double> dF, U;
+    std::vector<float> dFs, Us;
+    if (sp) {
+        dFs.assign((size_t)n * lda, 0.f);
+        Us.assign((size_t)n * lda, 0.f);
+    } else {
+        dF.assign((size_t)n * nhist, 0.0);
+        U.assign((size_t)n * nhist, 0.0);
+    }
+    converged = false;
+    int nstored = 0, nh = 0;
+    fmax = HUGE_VAL;
+    n_resets = 0;
+    for (int its = 1; its <= maxscf; its++) {
+        n_iter = its;
+        bool abort = false;
+        residual(n, x, F.data(), abort);
+        if (abort) break;
+        fmax = 0.0;
+        for (int64_t i = 0; i < n; i++) fmax = std::max(fmax, std::fabs(F[i]));
+        double rms = dnrm2(n, F.data()) / std::sqrt((double)n);
+        log.push_back({its, fmax, rms, std::min(nstored, nhist)});
+        if (fmax < tolf) {
+            converged = true;
+            break;
+        }
+        if (its > 1 && nhist > 0) {
+            int slot = nstored % nhist;  // 0-based
+            if (sp) {
+                for (int64_t i = 0; i < n; i++) Fold[i] = F[i] - Fold[i];
+                double fnorm = dnrm2(n, Fold.data());
+                if (fnorm > 0.0) {
+                    double rf = 1.0 / fnorm;
+                    float *dcol = &dFs[(size_t)n * slot], *ucol = &Us[(size_t)n * slot];
+#pragma omp parallel for
+                    for (int64_t i = 0; i < n; i++) {
+                        dcol[i] = (float)(Fold[i] * rf);
+                        ucol[i] = (float)(alpha_mix * Fold[i] * rf + (x[i] - xold[i]) * rf);
+                    }
+                    nstored++;
+                    nh = std::min(nstored, nhist);
+                    for (int k = 0; k < nh; k++) {
+                        const float *u = &dFs[(size_t)n * k];
+                        double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc)
+                        for (int64_t i = 0; i < n; i++) acc += (double)u[i] * (double)dcol[i];
+                        cvec[k] = acc;
+                    }
+                    for (int k = 0; k < nh; k++) {
+                        gram[k + (size_t)slot * lda] = cvec[k];
+                        gram[slot + (size_t)k * lda] = cvec[k];
+                    }
+                }
+            } else {
+                double *dcol = &dF[(size_t)n * slot], *ucol = &U[(size_t)n * slot];
+                for (int64_t i = 0; i < n; i++) dcol[i] = F[i] - Fold[i];
+                double fnorm = dnrm2(n, dcol);
+                if (fnorm > 0.0) {
+                    for (int64_t i = 0; i < n; i++) dcol[i] = dcol[i] / fnorm;
+                    for (int64_t i = 0; i < n; i++) ucol[i] = alpha_mix * dcol[i] + (x[i] - xold[i]) / fnorm;
+                    nstored++;
+                    nh = std::min(nstored, nhist);
+                    for (int k = 0; k < nh; k++) {
+                        const double *u = &dF[(size_t)n * k];
+                        double acc = 0.0;
+                        for (int64_t i = 0; i < n; i++) acc += u[i] * dcol[i];
+                        cvec[k] = acc;
+                    }
+                    for (int k = 0; k < nh; k++) {
+                        gram[k + (size_t)slot * lda] = cvec[k];
+                        gram[slot + (size_t)k * lda] = cvec[k];
+                    }
+                }
+            }
+        }
+        nh = std::min(nstored, nhist);
+        std::copy(x, x + n, xold.begin());
+        std::copy(F.begin(), F.end(), Fold.begin());
+        if (nh > 0) {
+            for (int j = 0; j < nh; j++)
+                for (int i = 0; i < nh; i++) a[i + (size_t)j * lda] = gram[i + (size_t)j * lda];
+            for (int i = 0; i < nh; i++) a[i + (size_t)i * lda] += w0 * w0;
+            for (int k = 0; k < nh; k++) {
+                double acc = 0.0;
+                if (sp) {
+                    const float *u = &dFs[(size_t)n * k];
+#pragma omp parallel for reduction(+ : acc)
+                    for (int64_t i = 0; i < n; i++) acc += (double)u[i] * F[i];
+                } else {
+                    const double *u = &dF[(size_t)n * k];
+                    for (int64_t i = 0; i < n; i++) acc += u[i] * F[i];
+                }
+                cvec[k] = acc;
+            }
+            int64_t nn = nh, one = 1, ld = lda, info = 0;
+            scipy_dposv_64_("U", &nn, &one, a.data(), &ld, cvec.data(), &ld, &info, 1);
+            if (info != 0) {
+                nstored = 0;
+                nh = 0;
+                n_resets++;
+            }
+        }
+        if (sp) {
+#pragma omp parallel for
+            for (int64_t i = 0; i < n; i++) {
+                double xi = x[i] + alpha_mix * F[i];
+                for (int k = 0; k < nh; k++) xi -= (double)Us[(size_t)n * k + i] * cvec[k];
+                x[i] = xi;
+            }
+        } else {
+            for (int64_t i = 0; i < n; i++) x[i] += alpha_mix * F[i];
+            if (nh > 0)
+                for (int k = 0; k < nh; k++) {
+                    const double *u = &U[(size_t)n * k];
+                    for (int64_t i = 0; i < n; i++) x[i] -= u[i] * cvec[k];
+                }
+        }
+    }
+}
+
+// final_sanity (src/scf.f90:260-275)
+static void final_sanity(qso_state &s, bool &runaway, bool &unphysical, int &i_worst, double &n_worst, double &w_worst) {
+    std::vector<cplx> grd((size_t)s.Norb * s.n), gld((size_t)s.Norb * s.n);
+    for (int iw = 0; iw < s.n; iw++)
+        for (int i = 1; i <= s.Norb; i++) {
+            int st = (i + 1) / 2, a = i - 2 * (st - 1);
+            grd[(i - 1) + (size_t)iw * s.Norb] = cplx(0.0, s.dosd[(i - 1) + (size_t)iw * s.Norb]);
+            gld[(i - 1) + (size_t)iw * s.Norb] = s.onsL[(size_t)(4 * (st - 1) + 2 * (a - 1) + a - 1) + (size_t)iw * 4 * s.N_sites];
+        }
+    check_diag_sanity(grd.data(), gld.data(), s.Norb, s.n, s.delta, runaway, unphysical, i_worst, n_worst, w_worst, nullptr);
+}
+
+static void hemb(qso_state &s) {
+    // Hemb = -H + (i/2 hbar)(GammaL + GammaR)   (src/scf.f90:92)
+    for (size_t k = 0; k < s.H.size(); k++) s.Hemb[k] = -s.H[k] + 0.5 * (IM / HBAR) * (s.GammaL[k] + s.GammaR[k]);
+}
+
+// ------------------------------------------------------------------------------------
+// C ABI (same signatures as include/qsb200.h, prefix qso_)
+// ------------------------------------------------------------------------------------
+extern "C" {
+
+int qso_create(const qs_problem *p, qso_state **out) {
+    scipy_openblas_set_num_threads64_(1);  // one LAPACK thread per OpenMP thread, as the reference runs
+    auto *s = new qso_state();
+    s->Norb = p->Norb;
+    s->N_sites = p->N_sites;
+    s->N_atoms = p->N_atoms;
+    s->order = p->order;
+    s->n = p->n_omega;
+    size_t nn = (size_t)p->Norb * p->Norb;
+    s->H.assign((const cplx *)p->H, (const cplx *)p->H + nn);
+    s->GammaL.assign((const cplx *)p->GammaL, (const cplx *)p->GammaL + nn);
+    s->GammaR.assign((const cplx *)p->GammaR, (const cplx *)p->GammaR + nn);
+    s->U_site.assign(p->U_site, p->U_site + p->Norb);
+    s->omega.assign(p->omega, p->omega + p->n_omega);
+    s->atom_norb.assign(p->atom_norb, p->atom_norb + p->N_atoms);
+    s->atom_first.assign(p->atom_first, p->atom_first + p->N_atoms);
+    s->mu = p->mu;
+    s->beta = p->beta;
+    s->delta = p->delta;
+    s->alpha_mix = p->alpha_mix;
+    s->tolf = p->tolf;
+    s->tolf_order1 = p->tolf_order1;
+    s->nhist = p->nhist;
+    s->maxscf = p->maxscf;
+    s->single_history = p->single_history != 0;
+    setup_storage(*s);
+    *out = s;
+    return 0;
+}
+
+void qso_destroy(qso_state *s) { delete s; }
+const char *qso_last_error(const qso_state *s) { return s ? s->err.c_str() : "no handle"; }
+int64_t qso_vector_length(const qso_state *s) { return s->n_vec; }
+int qso_active_states(const qso_state *s) { return s->nA; }
+int qso_fft_length(const qso_state *s) { return good_fft_size(2 * s->n - 1); }
+
+static int check_singular(qso_state *s) {
+    if (s->singular) {
+        s->err = "ERROR: ZGETRF failed (singular matrix?) at energy " + std::to_string(s->singular);
+        int e = (int)s->singular;
+        s->singular = 0;
+        return e;
+    }
+    return 0;
+}
+
+// solve_scf (src/scf.f90:78-151)
+int qso_solve_scf(qso_state *s, double Volt, int fresh_start, qs_scf_result *res) {
+    auto t0 = std::chrono::steady_clock::now();
+    hemb(*s);
+    s->V_scf = Volt;
+    s->scf_iter = 0;
+    bool converged = true;
+    int n_iter = 0, n_resets = 0;
+    double fmax = 0.0;
+    std::vector<qs_scf_step> log;
+    bool aborted = false;
+    if (s->order == 1) {
+        if (fresh_start || !s->have_x) {
+            std::fill(s->G_less_t0.begin(), s->G_less_t0.end(), 0.0);
+            s->use_sigma = false;
+            sweep(*s, M_SCF1, nullptr);
+            gather_onsite(*s, s->site_int, s->G_less_t0);
+        }
+        std::vector<double> x(s->n_vec);
+        pack_nil(*s, s->G_less_t0, x.data());
+        broyden_solve([&](int64_t n, const double *xx, double *F, bool &ab) { scf_residual1(*s, n, xx, F, ab); aborted = aborted || ab; },
+                      x.data(), s->n_vec, s->alpha_mix, s->nhist, s->maxscf, s->tolf_order1, s->single_history, converged,
+                      n_iter, fmax, log, n_resets);
+    } else if (s->order == 2) {
+        if (!s->sigma2_ready) sigma2_init(*s);
+        std::vector<double> x(s->n_vec);
+        if (fresh_start || !s->have_x) {
+            s->use_sigma = false;
+            sweep(*s, M_INIT2, nullptr);
+        }
+        pack_gf(s->Gr_in.data(), s->GL_in.data(), x.data(), s->n_full, s->n_strict_upper, s->nA, s->n);
+        broyden_solve([&](int64_t n, const double *xx, double *F, bool &ab) { scf_residual2(*s, n, xx, F, ab); aborted = aborted || ab; },
+                      x.data(), s->n_vec, s->alpha_mix, s->nhist, s->maxscf, s->tolf, s->single_history, converged, n_iter,
+                      fmax, log, n_resets);
+        s->have_x = true;
+    } else {
+        log.push_back({1, 0.0, 0.0, 0});
+        n_iter = 1;
+    }
+    if (s->order == 1) s->have_x = true;
+    if (int e = check_singular(s)) return e;
+    // final sweep with the converged self-energies (Sig1, SigR2, SigL2 of the last input)
+    s->use_sigma = (s->order >= 1);
+    sweep(*s, M_FINAL, nullptr);
+    if (int e = check_singular(s)) return e;
+    std::fill(s->G_less_obs.begin(), s->G_less_obs.end(), 0.0);
+    std::vector<char> all(s->N_sites + 1, 1);
+    gather_onsite(*s, all, s->G_less_obs);
+    gather_atoms(*s, s->G_less_obs);
+    bool runaway, unphysical;
+    int i_worst;
+    double n_worst, w_worst;
+    final_sanity(*s, runaway, unphysical, i_worst, n_worst, w_worst);
+    if (converged && unphysical) converged = false;
+    res->converged = converged;
+    res->n_iter = n_iter;
+    res->fmax = fmax;
+    res->aborted = aborted;
+    res->runaway = runaway;
+    res->unphysical = unphysical;
+    res->i_worst = i_worst;
+    res->n_worst = n_worst;
+    res->w_worst = w_worst;
+    res->n_resets = n_resets;
+    res->n_log = 0;
+    for (auto &e : log)
+        if (res->log && res->n_log < res->log_cap) res->log[res->n_log++] = e;
+    res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return 0;
+}
+
+// Current (src/observables.f90:22-39)
+int qso_current(qso_state *s, double, double *J_up, double *J_down) {
+    double ju = 0.0, jd = 0.0;
+    for (int iw = 0; iw < s->n; iw++) {
+        ju += s->trU[iw];
+        jd += s->trD[iw];
+    }
+    *J_up = ju * (s->delta / HBAR);
+    *J_down = jd * (s->delta / HBAR);
+    return 0;
+}
+
+int qso_get_observables(qso_state *s, double *G_less_obs, double *dosd, double *trU, double *trD) {
+    if (G_less_obs) std::memcpy(G_less_obs, s->G_less_obs.data(), sizeof(cplx) * s->G_less_obs.size());
+    if (dosd) std::memcpy(dosd, s->dosd.data(), sizeof(double) * s->dosd.size());
+    if (trU) std::memcpy(trU, s->trU.data(), sizeof(double) * s->n);
+    if (trD) std::memcpy(trD, s->trD.data(), sizeof(double) * s->n);
+    return 0;
+}
+
+int qso_initial_vector(qso_state *s, double Volt, double *x) {
+    hemb(*s);
+    s->V_scf = Volt;
+    if (s->order == 2) {
+        if (!s->sigma2_ready) sigma2_init(*s);
+        s->use_sigma = false;
+        sweep(*s, M_INIT2, nullptr);
+        pack_gf(s->Gr_in.data(), s->GL_in.data(), x, s->n_full, s->n_strict_upper, s->nA, s->n);
+    } else if (s->order == 1) {
+        std::fill(s->G_less_t0.begin(), s->G_less_t0.end(), 0.0);
+        s->use_sigma = false;
+        sweep(*s, M_SCF1, nullptr);
+        gather_onsite(*s, s->site_int, s->G_less_t0);
+        pack_nil(*s, s->G_less_t0, x);
+    }
+    return check_singular(s);
+}
+
+int qso_residual(qso_state *s, double Volt, const double *x, double *F, int *abort_flag) {
+    hemb(*s);
+    s->V_scf = Volt;
+    bool ab = false;
+    if (s->order == 2) {
+        if (!s->sigma2_ready) sigma2_init(*s);
+        scf_residual2(*s, s->n_vec, x, F, ab);
+    } else if (s->order == 1) {
+        scf_residual1(*s, s->n_vec, x, F, ab);
+    }
+    *abort_flag = ab;
+    return check_singular(s);
+}
+
+int qso_self_energies(qso_state *s, const double *x, double *SigR2, double *SigL2, double *Sig1) {
+    if (s->order != 2) return -1;
+    if (!s->sigma2_ready) sigma2_init(*s);
+    unpack_gf(s->Gr_in.data(), s->GL_in.data(), x, s->n_full, s->n_strict_upper, s->nA, s->n);
+    equal_time_lesser(*s);
+    sigma_first_order(*s);
+    sigma2_compute(*s, true);
+    if (SigR2) std::memcpy(SigR2, s->SigR2.data(), sizeof(cplx) * s->SigR2.size());
+    if (SigL2) std::memcpy(SigL2, s->SigL2.data(), sizeof(cplx) * s->SigL2.size());
+    if (Sig1) std::memcpy(Sig1, s->Sig1.data(), sizeof(cplx) * s->Sig1.size());
+    return 0;
+}
+
+int qso_invert_batched(int N, int batch, double *A, int *info, int) {
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : bad)
+    for (int b = 0; b < batch; b++) {
+        int64_t e = invert_complex(N, (cplx *)A + (size_t)b * N * N);
+        info[b] = (int)e;
+        bad += e != 0;
+    }
+    return bad ? 1 : 0;
+}
+
+int qso_pack_gf(int nb, int Nw, const double *Gr, const double *Gl, double *out) {
+    int nf = nb * nb, nsu = (nf - nb) / 2;
+    pack_gf((const cplx *)Gr, (const cplx *)Gl, out, nf, nsu, nb, Nw);
+    return 0;
+}
+int qso_unpack_gf(int nb, int Nw, const double *in, double *Gr, double *Gl) {
+    int nf = nb * nb, nsu = (nf - nb) / 2;
+    unpack_gf((cplx *)Gr, (cplx *)Gl, in, nf, nsu, nb, Nw);
+    return 0;
+}
+
+int qso_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t n, double alpha_mix, int nhist,
+                           int maxscf, double tolf, int single_history, int *converged, int *n_iter, double *fmax,
+                           qs_scf_step *log, int log_cap) {
+    bool conv = false;
+    int it = 0, resets = 0;
+    double fm = 0;
+    std::vector<qs_scf_step> lg;
+    broyden_solve(
+        [&](int64_t nn, const double *xx, double *F, bool &ab) {
+            int a = 0;
+            residual(ctx, nn, xx, F, &a);
+            ab = a != 0;
+        },
+        x, n, alpha_mix, nhist, maxscf, tolf, single_history != 0, conv, it, fm, lg, resets);
+    *converged = conv;
+    *n_iter = it;
+    *fmax = fm;
+    for (int i = 0; i < (int)lg.size() && i < log_cap; i++) log[i] = lg[i];
+    return 0;
+}
+
+// standalone FFT in the reference's convention (for the FFT pin against numpy)
+int qso_fft(int n, double *data, int sign) {
+    FFTPlan p;
+    p.init(n);
+    std::vector<cplx> w(n);
+    p.exec((cplx *)data, w.data(), sign);
+    return 0;
+}
+int qso_good_fft_size(int nmin) { return good_fft_size(nmin); }
+
+}  // extern "C"
