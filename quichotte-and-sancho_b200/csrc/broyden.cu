@@ -1,0 +1,300 @@
+// broyden.cu -- modified Broyden mixing (D.D. Johnson, PRB 38, 12807 (1988)) on device
+// vectors: broyden_solve (common/broyden_mixing.f90:51-184) with its history in HBM.
+//
+// Every O(n) step is an FP64 device reduction or update; the host sees only the scalars
+// it needs each step (max|F|, rms|F|, ||dF||, the nh x nh Gram column and dF^T F) and
+// solves the nh x nh system (nh <= nhist) as the reference's dposv does. One pass of
+// hist_update writes the new history column pair AND accumulates its Gram column and
+// dF^T F against the whole history, so each history column is read once per step for the
+// dots and once for the x update.
+//
+// x, xold, F, Fold are rotated by pointer swaps instead of the reference's copies
+// (xold = x, Fold = F), so the state after a step is the reference's.
+#include <algorithm>
+#include <cmath>
+
+#include "qs_common.cuh"
+
+namespace qs {
+
+constexpr int RED_BLOCKS = 1184;  // 148 SMs x 8
+constexpr int RED_THREADS = 256;
+constexpr int MAXH = 32;           // largest history length handled by the fused kernels
+
+static int red_blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(RED_BLOCKS, (n + RED_THREADS - 1) / RED_THREADS)); }
+
+// block reduction of NV doubles (sum), result in lane 0 of warp 0 via shared memory
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sh /* [NV][RED_THREADS/32] */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k * 32 + wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double x = threadIdx.x < nw ? sh[k * 32 + threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            v[k] = x;
+        }
+    }
+    __syncthreads();
+}
+
+// partials[b] = (max |F|, sum F^2, sum (F-Fold)^2)
+__global__ void vec_norms(const double *__restrict__ F, const double *__restrict__ Fold, int64_t n, double *__restrict__ part) {
+    __shared__ double sh[3 * 32];
+    double mx = 0.0, v[2] = {0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double f = F[i];
+        mx = fmax(mx, fabs(f));
+        v[0] = fma(f, f, v[0]);
+        if (Fold) {
+            double d = f - Fold[i];
+            v[1] = fma(d, d, v[1]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) sh[64 + (threadIdx.x >> 5)] = mx;
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sh[64 + w]);
+        part[3 * blockIdx.x + 0] = m;
+        part[3 * blockIdx.x + 1] = v[0];
+        part[3 * blockIdx.x + 2] = v[1];
+    }
+}
+
+// New history pair in slot `slot` plus the Gram column and dF^T F over nh <= NH columns
+// (common/broyden_mixing.f90:103-138,150-156). Single-precision history stores
+// real(dF/||dF||) and real(alpha dF/||dF|| + dx/||dF||); every dot accumulates in FP64.
+template <typename HT, int NH>
+__global__ void __launch_bounds__(256) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
+                                                   const double *__restrict__ x, const double *__restrict__ xold,
+                                                   int64_t n, double fnorm, double alpha, HT *__restrict__ dF,
+                                                   HT *__restrict__ U, int slot, int nh, int store,
+                                                   double *__restrict__ part) {
+    __shared__ double sh[2 * NH * 32];
+    double g[NH], c[NH];
+#pragma unroll
+    for (int k = 0; k < NH; k++) { g[k] = 0.0; c[k] = 0.0; }
+    const double rf = 1.0 / fnorm;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double f = F[i];
+        HT dnew = (HT)0;
+        if (store) {
+            double d = f - Fold[i];
+            double dx = x[i] - xold[i];
+            if (sizeof(HT) == 4) {
+                dnew = (HT)(d * rf);
+                U[(int64_t)slot * n + i] = (HT)(alpha * d * rf + dx * rf);
+            } else {  // double history: dF = (F - Fold)/fnorm, U = alpha dF + (x - xold)/fnorm
+                double dd = d / fnorm;
+                dnew = (HT)dd;
+                U[(int64_t)slot * n + i] = (HT)(alpha * dd + dx / fnorm);
+            }
+            dF[(int64_t)slot * n + i] = dnew;
+        }
+#pragma unroll
+        for (int k = 0; k < NH; k++) {
+            if (k < nh) {
+                double dk = (store && k == slot) ? (double)dnew : (double)dF[(int64_t)k * n + i];
+                g[k] = fma(dk, (double)dnew, g[k]);
+                c[k] = fma(dk, f, c[k]);
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NH; k++) {
+        double a = g[k], b = c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            sh[(2 * k) * 32 + wid] = a;
+            sh[(2 * k + 1) * 32 + wid] = b;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * nh; t += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += sh[t * 32 + w];
+        part[(int64_t)blockIdx.x * 2 * MAXH + t] = s;
+    }
+}
+
+template <typename HT>
+static void launch_hist(int nb, cudaStream_t st, const double *F, const double *Fold, const double *x, const double *xold,
+                        int64_t n, double fnorm, double alpha, HT *dF, HT *U, int slot, int nh, int store, double *part) {
+    if (nh <= 4)
+        hist_update<HT, 4><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+    else if (nh <= 8)
+        hist_update<HT, 8><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+    else if (nh <= 16)
+        hist_update<HT, 16><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+    else
+        hist_update<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+}
+
+// x_new = x + alpha F - sum_k gamma_k U_k   (common/broyden_mixing.f90:165-178)
+template <typename HT>
+__global__ void x_update(const double *__restrict__ x, const double *__restrict__ F, const HT *__restrict__ U,
+                         const double *__restrict__ gam, int nh, double alpha, int64_t n, double *__restrict__ xnew) {
+    __shared__ double gs[MAXH];
+    if (threadIdx.x < nh) gs[threadIdx.x] = gam[threadIdx.x];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double xi = x[i] + alpha * F[i];
+        for (int k = 0; k < nh; k++) xi -= (double)U[(int64_t)k * n + i] * gs[k];
+        xnew[i] = xi;
+    }
+}
+
+// deterministic sum of per-block partials: out[j] = op_b part[b*stride + j]
+__global__ void part_reduce(const double *__restrict__ part, int nb, int stride, int nv, int max_first,
+                            double *__restrict__ out) {
+    int j = threadIdx.x;
+    if (j >= nv) return;
+    double s = 0.0;
+    for (int b = 0; b < nb; b++) {
+        double v = part[(int64_t)b * stride + j];
+        s = (max_first && j == 0) ? fmax(s, v) : s + v;
+    }
+    out[j] = s;
+}
+
+// Cholesky solve of the nh x nh system (w0^2 I + dF^T dF) gamma = dF^T F, as dposv('U').
+// Returns 0 or the LAPACK-style info (> 0: not positive definite).
+static int chol_solve(int nh, const std::vector<double> &A0, int lda, std::vector<double> &b) {
+    std::vector<double> U((size_t)nh * nh, 0.0);
+    for (int j = 0; j < nh; j++) {
+        double s = A0[j + (size_t)j * lda];
+        for (int k = 0; k < j; k++) s -= U[k + (size_t)j * nh] * U[k + (size_t)j * nh];
+        if (!(s > 0.0)) return j + 1;
+        double ujj = std::sqrt(s);
+        U[j + (size_t)j * nh] = ujj;
+        for (int i = j + 1; i < nh; i++) {
+            double t = A0[j + (size_t)i * lda];
+            for (int k = 0; k < j; k++) t -= U[k + (size_t)j * nh] * U[k + (size_t)i * nh];
+            U[j + (size_t)i * nh] = t / ujj;
+        }
+    }
+    for (int i = 0; i < nh; i++) {  // U^T y = b
+        double s = b[i];
+        for (int k = 0; k < i; k++) s -= U[k + (size_t)i * nh] * b[k];
+        b[i] = s / U[i + (size_t)i * nh];
+    }
+    for (int i = nh - 1; i >= 0; i--) {  // U x = y
+        double s = b[i];
+        for (int k = i + 1; k < nh; k++) s -= U[i + (size_t)k * nh] * b[k];
+        b[i] = s / U[i + (size_t)i * nh];
+    }
+    return 0;
+}
+
+int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *&d_F, double *&d_Fold, double *&d_xold,
+                      void *d_hdF, void *d_hU, int64_t n, double alpha_mix, int nhist, int maxscf, double tolf, bool sp,
+                      BroydenOut &out) {
+    const double w0 = 0.01;  // Johnson's regulariser
+    if (nhist > MAXH) {
+        h->err = "nhist larger than " + std::to_string(MAXH) + " is not supported";
+        return -1;
+    }
+    const int lda = std::max(nhist, 1);
+    std::vector<double> gram((size_t)lda * lda, 0.0), a((size_t)lda * lda), cvec(lda);
+    const int nb = red_blocks(n);
+    double *part = h->d_red, *fin = h->d_red + (size_t)RED_BLOCKS * 2 * MAXH;
+    double *gam = fin + 2 * MAXH;
+    std::vector<double> hv(2 * MAXH + 4);
+    int nstored = 0, nh = 0;
+    out = BroydenOut{};
+    out.fmax = HUGE_VAL;
+    cudaStream_t st = h->stream;
+    for (int its = 1; its <= maxscf; its++) {
+        out.n_iter = its;
+        bool abort = false;
+        int rc = res(d_x, d_F, abort);
+        if (rc) return rc;
+        if (abort) {
+            out.aborted = true;
+            break;
+        }
+        // max|F|, ||F||, ||F - Fold||
+        const bool want_dn = its > 1 && nhist > 0;
+        vec_norms<<<nb, RED_THREADS, 0, st>>>(d_F, want_dn ? d_Fold : nullptr, n, part);
+        part_reduce<<<1, 32, 0, st>>>(part, nb, 3, 3, 1, fin);
+        QS_CUDA(h, cudaGetLastError());
+        QS_CUDA(h, cudaMemcpyAsync(hv.data(), fin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        QS_CUDA(h, cudaStreamSynchronize(st));
+        double fmax = hv[0], rms = std::sqrt(hv[1]) / std::sqrt((double)n), fnorm = std::sqrt(hv[2]);
+        out.fmax = fmax;
+        out.log.push_back({its, fmax, rms, std::min(nstored, nhist)});
+        if (fmax < tolf) {
+            out.converged = true;
+            break;
+        }
+        // history pair, Gram column, dF^T F
+        bool store = want_dn && fnorm > 0.0;
+        int slot = want_dn ? nstored % nhist : 0;
+        int nh_new = store ? std::min(nstored + 1, nhist) : std::min(nstored, nhist);
+        if (nh_new > 0 || store) {
+            if (sp)
+                launch_hist<float>(nb, st, d_F, d_Fold, d_x, d_xold, n, store ? fnorm : 1.0, alpha_mix, (float *)d_hdF,
+                                   (float *)d_hU, slot, nh_new, store, part);
+            else
+                launch_hist<double>(nb, st, d_F, d_Fold, d_x, d_xold, n, store ? fnorm : 1.0, alpha_mix, (double *)d_hdF,
+                                    (double *)d_hU, slot, nh_new, store, part);
+            part_reduce<<<1, 2 * MAXH, 0, st>>>(part, nb, 2 * MAXH, 2 * nh_new, 0, fin);
+            QS_CUDA(h, cudaGetLastError());
+            QS_CUDA(h, cudaMemcpyAsync(hv.data(), fin, 2 * nh_new * sizeof(double), cudaMemcpyDeviceToHost, st));
+            QS_CUDA(h, cudaStreamSynchronize(st));
+        }
+        if (store) {
+            nstored++;
+            for (int k = 0; k < nh_new; k++) {
+                gram[k + (size_t)slot * lda] = hv[2 * k];
+                gram[slot + (size_t)k * lda] = hv[2 * k];
+            }
+        }
+        nh = std::min(nstored, nhist);
+        for (int k = 0; k < nh; k++) cvec[k] = hv[2 * k + 1];
+        // gamma = (w0^2 I + dF^T dF)^-1 dF^T F
+        if (nh > 0) {
+            for (int j = 0; j < nh; j++)
+                for (int i = 0; i < nh; i++) a[i + (size_t)j * lda] = gram[i + (size_t)j * lda];
+            for (int i = 0; i < nh; i++) a[i + (size_t)i * lda] += w0 * w0;
+            std::vector<double> b(cvec.begin(), cvec.begin() + nh);
+            if (chol_solve(nh, a, lda, b) != 0) {
+                nstored = 0;  // WARNING: Broyden history ill-conditioned, resetting
+                nh = 0;
+                out.n_resets++;
+            } else {
+                QS_CUDA(h, cudaMemcpyAsync(gam, b.data(), nh * sizeof(double), cudaMemcpyHostToDevice, st));
+            }
+        }
+        // x_new into the xold buffer, then rotate: xold <- x, x <- x_new, Fold <- F
+        if (sp)
+            x_update<float><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const float *)d_hU, gam, nh, alpha_mix, n, d_xold);
+        else
+            x_update<double><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const double *)d_hU, gam, nh, alpha_mix, n, d_xold);
+        QS_CUDA(h, cudaGetLastError());
+        std::swap(d_x, d_xold);
+        std::swap(d_F, d_Fold);
+    }
+    return 0;
+}
+
+size_t broyden_red_len() { return (size_t)RED_BLOCKS * 2 * MAXH + 4 * MAXH; }
+
+}  // namespace qs

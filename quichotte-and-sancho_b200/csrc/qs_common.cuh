@@ -1,0 +1,204 @@
+// qs_common.cuh -- shared definitions of the B200 NEGF solver.
+//
+// Device data layout (HBM), with nA active states, n energies, Nf padded FFT length:
+//   X, F, Fold, xold   SCF vectors, energy-major: block w (3 nA^2 doubles) holds
+//                      [ G^r  nA^2 complex, column-major, (re,im) interleaved
+//                      | G^< strict upper triangle, column by column, complex
+//                      | Im G^<_ii, nA doubles ].
+//                      This is a fixed permutation of the reference's pack_gf block
+//                      (common/linear_algebra.f90:155-191), so every Broyden quantity
+//                      (norms, dots, updates) is the reference's up to summation order.
+//   SigR, SigL         Sigma2^r, Sigma2^< as n blocks of nA x nA complex, column-major
+//                      (the reference's SigR2(nA,nA,n_omega)).
+//   Y, V               FFT intermediates, sequence-major: sequence s holds Nf complex
+//                      values ordered [l1][m2] of the four-step split Nf = N1*N2.
+//   gRd, gLd           diagonals (n x nA complex) for the sanity check.
+//   onsL, dosd, atomL, trU, trD   final-sweep arrays, energy-major (reference layout).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "qsb200.h"
+
+namespace qs {
+
+template <typename T>
+struct __align__(2 * sizeof(T)) cplx {
+    T x, y;
+};
+using zc = cplx<double>;
+using cc = cplx<float>;
+
+template <typename T> __host__ __device__ __forceinline__ cplx<T> mk(T a, T b) { return cplx<T>{a, b}; }
+template <typename T> __host__ __device__ __forceinline__ cplx<T> operator+(cplx<T> a, cplx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T> __host__ __device__ __forceinline__ cplx<T> operator-(cplx<T> a, cplx<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T> __host__ __device__ __forceinline__ cplx<T> operator-(cplx<T> a) { return {-a.x, -a.y}; }
+template <typename T> __host__ __device__ __forceinline__ cplx<T> operator*(cplx<T> a, cplx<T> b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename T> __host__ __device__ __forceinline__ cplx<T> operator*(T s, cplx<T> a) { return {s * a.x, s * a.y}; }
+template <typename T> __host__ __device__ __forceinline__ cplx<T> conj(cplx<T> a) { return {a.x, -a.y}; }
+// a += b*c (complex fused multiply-add)
+template <typename T> __host__ __device__ __forceinline__ void cfma(cplx<T> &a, cplx<T> b, cplx<T> c) {
+    a.x = fma(b.x, c.x, a.x);
+    a.x = fma(-b.y, c.y, a.x);
+    a.y = fma(b.x, c.y, a.y);
+    a.y = fma(b.y, c.x, a.y);
+}
+// a += b*conj(c)
+template <typename T> __host__ __device__ __forceinline__ void cfma_conj(cplx<T> &a, cplx<T> b, cplx<T> c) {
+    a.x = fma(b.x, c.x, a.x);
+    a.x = fma(b.y, c.y, a.x);
+    a.y = fma(-b.x, c.y, a.y);
+    a.y = fma(b.y, c.x, a.y);
+}
+template <typename T> __host__ __device__ __forceinline__ T cabs1(cplx<T> a) { return fabs(a.x) + fabs(a.y); }
+// 1/a by Smith's method (no overflow for |a| near the range limits)
+template <typename T> __device__ __forceinline__ cplx<T> crecip(cplx<T> a) {
+    if (fabs(a.x) >= fabs(a.y)) {
+        T r = a.y / a.x, d = a.x + a.y * r;
+        return {T(1) / d, -r / d};
+    } else {
+        T r = a.x / a.y, d = a.y + a.x * r;
+        return {r / d, T(-1) / d};
+    }
+}
+template <typename D, typename S> __host__ __device__ __forceinline__ cplx<D> cvt(cplx<S> a) { return {(D)a.x, (D)a.y}; }
+
+constexpr double PI = 3.14159265358979323846;
+constexpr int SMEM_MAX = 232448;  // max dynamic shared memory per block on sm_100 (227 KB)
+
+// The Gauss-Jordan kernel keeps the N x N complex matrix in shared memory when it fits
+// next to its ~1.3 KB of static shared memory (N <= 120 in FP64).
+inline bool dyson_fits_smem(int N) { return (size_t)N * N * 16 + 1536 <= (size_t)SMEM_MAX; }
+
+// FFT plan of one length L that divides Nf (radices applied in order).
+struct FftLen {
+    int L;
+    int nrad;
+    int rad[24];
+};
+
+// Stockham plan for Nf = N1 * N2 and the twiddle table W[k] = exp(-2 pi i k / Nf).
+struct FftPlan {
+    int Nf, N1, N2;
+    FftLen p1, p2;
+};
+
+// ---------------------------------------------------------------------------------
+// The solver handle (one per qs_create).
+// ---------------------------------------------------------------------------------
+struct DeviceBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace qs
+
+struct qs_handle {
+    // problem (host copies)
+    int Norb = 0, N_sites = 0, N_atoms = 0, order = 0, n = 0, device = 0, precision = 0;
+    double mu = 0, beta = 0, delta = 0, alpha_mix = 0.5, tolf = 1e-6, tolf_order1 = 1e-8;
+    int nhist = 16, maxscf = 300;
+    bool single = true;
+    std::vector<double> H, GammaL, GammaR, U_site, omega;  // complex arrays as double pairs
+    std::vector<int> atom_norb, atom_first;
+    // active subspace (setup_storage), 0-based indices
+    int nA = 0, nS = 0, nCL = 0, nAs = 0, n_int_sites = 0;
+    std::vector<int> act, pos, sup, cl, asite;
+    std::vector<char> site_int, site_act;
+    bool has_atomL = false;
+    std::vector<int> atom_off;
+    int64_t n_vec = 0, nblk = 0;
+    // device model arrays
+    qs::zc *d_Hemb = nullptr, *d_Sig1 = nullptr, *d_GamLs = nullptr, *d_GamRs = nullptr, *d_GamLcl = nullptr;
+    int *d_pos = nullptr;
+    int *d_act = nullptr, *d_sup = nullptr, *d_cl = nullptr, *d_atom_first = nullptr, *d_atom_norb = nullptr,
+        *d_atom_off = nullptr, *d_site_int = nullptr;
+    double *d_omega = nullptr, *d_U = nullptr;
+    // SCF vectors and Broyden history (order 2: n_vec doubles; order 1: tiny)
+    double *d_x = nullptr, *d_F = nullptr, *d_Fold = nullptr, *d_xold = nullptr;
+    void *d_hdF = nullptr, *d_hU = nullptr;  // nhist columns, float (single history) or double
+    // second-order self-energies and the FFT
+    qs::FftPlan fft{};
+    qs::zc *d_tw = nullptr;  // Nf twiddles
+    qs::zc *d_SigR = nullptr, *d_SigL = nullptr;
+    qs::zc *d_Y = nullptr, *d_V = nullptr;
+    size_t nY = 0, nV = 0;
+    int2 *d_ydesc = nullptr;  // per Y sequence: offsets of (re, im) in a DL block (-1 = zero)
+    double *sig2_Upair = nullptr;  // U_I U_J hbar^2 (delta/2pi)^2 / Nf per site pair
+    int2 *sig2_pairs = nullptr;    // interacting site pairs I <= J
+    int sig2_npairs = 0, sig2_SA = 1, sig2_GA = 1, sig2_GC = 1;
+    size_t sig2_smem[3] = {0, 0, 0};
+    // sweep scratch
+    qs::zc *d_G = nullptr;  // Dyson output (G_AA for all energies, or full G for a chunk)
+    size_t G_chunk = 0;     // energies per chunk in full-G mode
+    qs::zc *d_T = nullptr;  // per-CTA GEMM scratch
+    size_t T_slots = 0, T_bytes = 0;
+    qs::zc *d_Gws = nullptr;  // Gauss-Jordan workspace when N x N does not fit in shared memory
+    size_t ws_slots = 0;
+    qs::zc *d_gRd = nullptr, *d_gLd = nullptr, *d_onsL = nullptr, *d_atomL = nullptr;
+    double *d_dosd = nullptr, *d_trU = nullptr, *d_trD = nullptr;
+    qs::zc *d_Glt0 = nullptr;  // G^<(t=0) on-site blocks, 4 per site
+    double *d_red = nullptr;   // reduction scratch
+    size_t red_len = 0;
+    int *d_info = nullptr;     // first singular energy (+1), 0 if none
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // host state
+    std::vector<double> G_less_t0, G_less_obs, Sig1;  // Norb*Norb complex
+    double J_up = 0, J_down = 0;
+    bool have_x = false, final_done = false;
+    std::vector<double> x1_host;  // order-1 SCF vector
+    std::string err;
+    size_t bytes_allocated = 0;
+    std::vector<void *> allocs;
+};
+
+namespace qs {
+
+// error handling: every CUDA call inside the library goes through this
+#define QS_CUDA(h, call)                                                                        \
+    do {                                                                                        \
+        cudaError_t _e = (call);                                                                \
+        if (_e != cudaSuccess) {                                                                \
+            (h)->err = std::string(#call) + ": " + cudaGetErrorString(_e);                      \
+            return -(int)_e;                                                                     \
+        }                                                                                       \
+    } while (0)
+
+int dalloc(qs_handle *h, void **p, size_t bytes);
+
+// launchers (implemented in the .cu files)
+int sigma2_setup(qs_handle *h);
+int sigma2_compute(qs_handle *h, const double *d_x);
+int equal_time_lesser_sigma1(qs_handle *h, const double *d_x);
+enum SweepMode { M_INIT2 = 1, M_SCF2 = 2, M_SCF1 = 3, M_FINAL = 4 };
+int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x);
+int sum_over_energies(qs_handle *h, const zc *d_A, int64_t ld, int ncols, int64_t nrows, zc *d_out);
+int sum_over_energies_real(qs_handle *h, const double *d_A, int64_t ld, int ncols, int64_t nrows, double *d_out);
+int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, zc *d_ws, int ws_slots);
+int convert_ref_to_dl(cudaStream_t st, int nA, int64_t Nw, const double *ref, double *dl);
+int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, double *ref);
+
+// Broyden (common/broyden_mixing.f90) on device vectors; the residual is a host callback
+// that fills F (device) from x (device) and may set abort.
+struct BroydenResidual {
+    virtual int operator()(const double *d_x, double *d_F, bool &abort) = 0;
+    virtual ~BroydenResidual() = default;
+};
+struct BroydenOut {
+    bool converged = false;
+    int n_iter = 0, n_resets = 0;
+    double fmax = 0;
+    bool aborted = false;
+    std::vector<qs_scf_step> log;
+};
+int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *&d_F, double *&d_Fold,
+                      double *&d_xold, void *d_hdF, void *d_hU, int64_t n, double alpha_mix, int nhist, int maxscf,
+                      double tolf, bool sp, BroydenOut &out);
+
+}  // namespace qs

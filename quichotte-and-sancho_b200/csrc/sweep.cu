@@ -1,0 +1,631 @@
+// sweep.cu -- the energy sweep (sweep / G_at_energy, src/scf.f90:280-415) as batched
+// kernels over the whole energy grid:
+//   dyson_gj        G^r(w) = [hbar w - H + (i/2hbar)(GammaL+GammaR) - Sigma^r(w)]^-1 by
+//                   in-place Gauss-Jordan elimination with partial pivoting, one thread
+//                   block per energy, the matrix staged in shared memory (global
+//                   workspace when N^2 complex does not fit), pivot search by warp
+//                   shuffles (invert_complex, common/linear_algebra.f90:58-88)
+//   keldysh_scf2    G^< = G^r Sigma^< G^a on the active block as two complex GEMMs per
+//                   energy, written straight into the SCF vector with its diagonals
+//                   (modes M_INIT2 / M_SCF2, src/scf.f90:340-355)
+//   final_outputs   modes M_SCF1 / M_FINAL (src/scf.f90:357-410): on-site and intra-atom
+//                   blocks of G^<, Im G^r_ii, the current integrand
+// plus the reductions over energies (equal_time_lesser, gather_onsite, gather_atoms,
+// Current, the sanity sums) and the pack_gf / unpack_gf layout conversions.
+#include <algorithm>
+#include <cmath>
+
+#include "qs_common.cuh"
+
+namespace qs {
+
+__device__ __forceinline__ double fermi_d(double w, double V, double mu, double beta) {
+    // src/green_functions.f90:74-84 (hbar = 1)
+    double arg = (w - mu + V) * beta;
+    return 1.0 / (exp(fmin(arg, 700.0)) + 1.0);
+}
+
+// ---------------------------------------------------------------------------------
+// Block-wide argmax of cabs1 over rows k..N-1 of column k (first maximum wins, as
+// LAPACK's izamax).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void warp_argmax(double &v, int &i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_down_sync(0xffffffffu, v, o);
+        int i2 = __shfl_down_sync(0xffffffffu, i, o);
+        if (v2 > v || (v2 == v && i2 < i)) {
+            v = v2;
+            i = i2;
+        }
+    }
+}
+
+struct DysonArgs {
+    int N, nA, iw0, iw1;
+    const zc *Hemb, *Sig1, *SigR;
+    const int *pos;  // full index -> active index, -1 if inactive
+    const int *act;
+    const double *omega;
+    int use_sigma, order2;
+    int out_mode;  // 0: G_AA for energy iw at Gout[iw*nA^2]; 1: full G at Gout[(iw-iw0)*N^2]
+    zc *Gout;
+    zc *ws;        // global workspace (N^2 per block) when the matrix is not in shared memory
+    int *info;     // min over energies of (iw + 1) with a zero pivot; INT_MAX if none
+    const zc *Ain; // batched-inversion mode: matrices to invert (nullptr for the sweep)
+    int *info_each;
+};
+
+__global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N = a.N;
+    const bool in_smem = (a.ws == nullptr);
+    zc *M = in_smem ? (zc *)smem_raw : a.ws + (size_t)blockIdx.x * N * N;
+    __shared__ unsigned short perm[512];
+    __shared__ double wv[16];
+    __shared__ int wi[16];
+    __shared__ int piv_s;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int NG = nthr / N;  // threads per row in the update (>= 1, N <= 512)
+    const int myrow = tid % N, mygrp = tid / N;
+    const bool upd = mygrp < NG;
+
+    for (int iw = a.iw0 + blockIdx.x; iw < a.iw1; iw += gridDim.x) {
+        // ---- build w1 = Hemb - (Sig1 + Sigma2^r(w)) on act x act, + hbar w on the diagonal
+        if (a.Ain) {
+            const zc *A = a.Ain + (size_t)(iw - a.iw0) * N * N;
+            for (int idx = tid; idx < N * N; idx += nthr) M[idx] = A[idx];
+        } else {
+            const double w = a.omega[iw];
+            const zc *SR = a.SigR + (size_t)iw * a.nA * a.nA;
+            for (int idx = tid; idx < N * N; idx += nthr) {
+                int i = idx % N, j = idx / N;
+                zc v = a.Hemb[idx];
+                if (a.use_sigma) {
+                    int pi = a.pos[i], pj = a.pos[j];
+                    if (pi >= 0 && pj >= 0) {
+                        zc s = a.Sig1[idx];
+                        if (a.order2) s = s + SR[pi + (size_t)pj * a.nA];
+                        v = v - s;
+                    }
+                }
+                if (i == j) v.x += w;
+                M[idx] = v;
+            }
+        }
+        __syncthreads();
+        bool singular = false;
+        // ---- Gauss-Jordan with row interchanges
+        for (int k = 0; k < N; k++) {
+            // pivot search
+            double v = -1.0;
+            int vi = N;
+            for (int i = k + tid; i < N; i += nthr) {
+                double c = cabs1(M[i + (size_t)k * N]);
+                if (c > v) { v = c; vi = i; }
+            }
+            warp_argmax(v, vi);
+            if ((tid & 31) == 0) { wv[tid >> 5] = v; wi[tid >> 5] = vi; }
+            __syncthreads();
+            if (tid < 32) {
+                int nw = nthr >> 5;
+                v = tid < nw ? wv[tid] : -1.0;
+                vi = tid < nw ? wi[tid] : N;
+                warp_argmax(v, vi);
+                if (tid == 0) { piv_s = vi; perm[k] = vi; }
+            }
+            __syncthreads();
+            const int p = piv_s;
+            if (p != k) {
+                for (int j = tid; j < N; j += nthr) {
+                    zc t = M[k + (size_t)j * N];
+                    M[k + (size_t)j * N] = M[p + (size_t)j * N];
+                    M[p + (size_t)j * N] = t;
+                }
+                __syncthreads();
+            }
+            zc pivot = M[k + (size_t)k * N];
+            if (pivot.x == 0.0 && pivot.y == 0.0) singular = true;
+            zc inv = singular ? zc{0.0, 0.0} : crecip(pivot);
+            zc f = upd ? M[myrow + (size_t)k * N] : zc{0.0, 0.0};
+            __syncthreads();
+            // scale the pivot row (M[k][k] is replaced by 1 first, so it ends as 1/pivot)
+            for (int j = tid; j < N; j += nthr) {
+                zc t = (j == k) ? zc{1.0, 0.0} : M[k + (size_t)j * N];
+                M[k + (size_t)j * N] = t * inv;
+            }
+            __syncthreads();
+            // rank-1 update of every other row (column k is replaced by 0 first)
+            if (upd && myrow != k) {
+                for (int j = mygrp; j < N; j += NG) {
+                    zc t = (j == k) ? zc{0.0, 0.0} : M[myrow + (size_t)j * N];
+                    zc r = M[k + (size_t)j * N];
+                    t.x = fma(-f.x, r.x, t.x);
+                    t.x = fma(f.y, r.y, t.x);
+                    t.y = fma(-f.x, r.y, t.y);
+                    t.y = fma(-f.y, r.x, t.y);
+                    M[myrow + (size_t)j * N] = t;
+                }
+            }
+            __syncthreads();
+        }
+        // undo the row interchanges by column interchanges in reverse order
+        if (tid < N) {
+            for (int k = N - 1; k >= 0; k--) {
+                int p = perm[k];
+                if (p != k) {
+                    zc t = M[tid + (size_t)k * N];
+                    M[tid + (size_t)k * N] = M[tid + (size_t)p * N];
+                    M[tid + (size_t)p * N] = t;
+                }
+            }
+        }
+        __syncthreads();
+        if (singular && tid == 0) {
+            atomicMin(a.info, iw + 1);
+            if (a.info_each) a.info_each[iw - a.iw0] = 1;
+        }
+        // ---- output
+        if (a.out_mode == 0) {
+            const int nA = a.nA;
+            zc *G = a.Gout + (size_t)iw * nA * nA;
+            for (int idx = tid; idx < nA * nA; idx += nthr) {
+                int p = idx % nA, q = idx / nA;
+                G[idx] = M[a.act[p] + (size_t)a.act[q] * N];
+            }
+        } else {
+            zc *G = a.Gout + (size_t)(iw - a.iw0) * N * N;
+            for (int idx = tid; idx < N * N; idx += nthr) G[idx] = M[idx];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Block-level complex GEMM C(MxN) = A(MxK) B(KxN) over 32x32 output tiles, 256 threads,
+// each thread 2x2 outputs. Operands come from loader functors; the store functor gets
+// (i, j, value). With `upper`, tiles strictly below the diagonal are skipped.
+// ---------------------------------------------------------------------------------
+constexpr int TB = 32, TK = 16;
+
+template <class LA, class LB, class ST>
+__device__ void cta_gemm(int M, int N, int K, LA la, LB lb, ST st, zc *sA, zc *sB, bool upper) {
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int mt = (M + TB - 1) / TB, nt = (N + TB - 1) / TB;
+    for (int tile = 0; tile < mt * nt; tile++) {
+        const int bi = tile % mt, bj = tile / mt;
+        if (upper && bi > bj) continue;
+        zc acc[2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
+        for (int k0 = 0; k0 < K; k0 += TK) {
+            // sA[kk][r] (TK x TB), sB[kk][c] (TK x TB)
+            for (int idx = tid; idx < TB * TK; idx += 256) {
+                int r = idx % TB, kk = idx / TB;
+                int i = bi * TB + r, k = k0 + kk;
+                sA[kk * TB + r] = (i < M && k < K) ? la(i, k) : zc{0, 0};
+            }
+            for (int idx = tid; idx < TB * TK; idx += 256) {
+                int kk = idx % TK, c = idx / TK;
+                int j = bj * TB + c, k = k0 + kk;
+                sB[kk * TB + c] = (j < N && k < K) ? lb(k, j) : zc{0, 0};
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < TK; kk++) {
+                zc a0 = sA[kk * TB + ty], a1 = sA[kk * TB + ty + 16];
+                zc b0 = sB[kk * TB + tx], b1 = sB[kk * TB + tx + 16];
+                cfma(acc[0][0], a0, b0);
+                cfma(acc[0][1], a0, b1);
+                cfma(acc[1][0], a1, b0);
+                cfma(acc[1][1], a1, b1);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                int i = bi * TB + ty + 16 * r, j = bj * TB + tx + 16 * c;
+                if (i < M && j < N) st(i, j, acc[r][c]);
+            }
+    }
+}
+
+struct KeldyshArgs {
+    int nA, n;
+    int64_t nblk;
+    const zc *G;     // G_AA per energy (nA^2 complex)
+    const zc *SigL;  // Sigma2^< per energy, or nullptr
+    const zc *GamLs, *GamRs;
+    const double *omega;
+    double V, mu, beta;
+    double *out;        // DL blocks (SCF vector)
+    const double *xsub; // subtracted (F = out - x), or nullptr
+    zc *gRd, *gLd;      // diagonals, or nullptr
+    zc *Tws;            // per-block scratch, nA^2 complex
+};
+
+// modes M_INIT2 / M_SCF2: T = G^r SL, G^< = T G^r^dagger (upper triangle), packed.
+__global__ void __launch_bounds__(256) keldysh_scf2(KeldyshArgs a) {
+    __shared__ zc sA[TB * TK], sB[TB * TK];
+    const int nA = a.nA, nfull = nA * nA;
+    zc *T = a.Tws + (size_t)blockIdx.x * nfull;
+    for (int iw = blockIdx.x; iw < a.n; iw += gridDim.x) {
+        const zc *G = a.G + (size_t)iw * nfull;
+        const double w = a.omega[iw];
+        const double fL = fermi_d(w, a.V, a.mu, a.beta), fR = fermi_d(w, 0.0, a.mu, a.beta);
+        const zc *SL2 = a.SigL ? a.SigL + (size_t)iw * nfull : nullptr;
+        // SL = i (fL GamL_s + fR GamR_s) / hbar  (+ Sigma2^<)   (src/scf.f90:333-336)
+        auto ldSL = [&](int k, int j) {
+            size_t idx = k + (size_t)j * nA;
+            zc g{fL * a.GamLs[idx].x + fR * a.GamRs[idx].x, fL * a.GamLs[idx].y + fR * a.GamRs[idx].y};
+            zc s{-g.y, g.x};
+            if (SL2) s = s + SL2[idx];
+            return s;
+        };
+        cta_gemm(
+            nA, nA, nA, [&](int i, int k) { return G[i + (size_t)k * nA]; }, ldSL,
+            [&](int i, int j, zc v) { T[i + (size_t)j * nA] = v; }, sA, sB, false);
+        __syncthreads();
+        double *blk = a.out + (size_t)iw * a.nblk;
+        const double *xb = a.xsub ? a.xsub + (size_t)iw * a.nblk : nullptr;
+        const int64_t offL = 2 * (int64_t)nfull, offD = offL + (int64_t)nA * (nA - 1);
+        cta_gemm(
+            nA, nA, nA, [&](int i, int k) { return T[i + (size_t)k * nA]; },
+            [&](int k, int j) { return conj(G[j + (size_t)k * nA]); },
+            [&](int i, int j, zc v) {
+                if (i < j) {
+                    int64_t o = offL + 2 * ((int64_t)j * (j - 1) / 2 + i);
+                    blk[o] = xb ? v.x - xb[o] : v.x;
+                    blk[o + 1] = xb ? v.y - xb[o + 1] : v.y;
+                } else if (i == j) {
+                    blk[offD + i] = xb ? v.y - xb[offD + i] : v.y;
+                    if (a.gLd) a.gLd[(size_t)iw * nA + i] = v;
+                }
+            },
+            sA, sB, true);
+        // G^r part of the block
+        for (int idx = threadIdx.x; idx < nfull; idx += blockDim.x) {
+            zc g = G[idx];
+            blk[2 * idx] = xb ? g.x - xb[2 * idx] : g.x;
+            blk[2 * idx + 1] = xb ? g.y - xb[2 * idx + 1] : g.y;
+            int i = idx % nA, j = idx / nA;
+            if (i == j && a.gRd) a.gRd[(size_t)iw * nA + i] = g;
+        }
+        __syncthreads();
+    }
+}
+
+struct FinalArgs {
+    int N, nS, nA, nCL, N_sites, N_atoms, iw0, iw1, mode;
+    const zc *G;  // full G per energy of the chunk
+    const int *sup, *act, *pos, *cl, *site_int, *atom_first, *atom_norb, *atom_off;
+    const zc *GamLs, *GamRs, *GamLcl, *SigL;
+    const double *omega;
+    double V, mu, beta;
+    zc *Tws;
+    double *dosd, *trU, *trD;
+    zc *onsL, *atomL, *gRd, *gLd;
+    int atomL_ld;
+};
+
+// modes M_SCF1 and M_FINAL (src/scf.f90:357-410)
+__global__ void __launch_bounds__(256) final_outputs(FinalArgs a) {
+    __shared__ zc sA[TB * TK], sB[TB * TK];
+    __shared__ zc Xs[32 * 32];  // nCL <= 32 (checked in qs_create)
+    const int N = a.N, nS = a.nS;
+    const bool fin = (a.mode == M_FINAL);
+    const int Mrows = fin ? N : a.nA;
+    zc *T = a.Tws + (size_t)blockIdx.x * Mrows * nS;
+    for (int iw = a.iw0 + blockIdx.x; iw < a.iw1; iw += gridDim.x) {
+        const zc *G = a.G + (size_t)(iw - a.iw0) * N * N;
+        auto g = [&](int i, int j) { return G[i + (size_t)j * N]; };
+        const double w = a.omega[iw];
+        const double fL = fermi_d(w, a.V, a.mu, a.beta), fR = fermi_d(w, 0.0, a.mu, a.beta);
+        const zc *SL2 = a.SigL ? a.SigL + (size_t)iw * a.nA * a.nA : nullptr;
+        auto ldSL = [&](int k, int j) {
+            size_t idx = k + (size_t)j * nS;
+            zc gg{fL * a.GamLs[idx].x + fR * a.GamRs[idx].x, fL * a.GamLs[idx].y + fR * a.GamRs[idx].y};
+            zc s{-gg.y, gg.x};
+            if (SL2) s = s + SL2[idx];
+            return s;
+        };
+        // T = w1(rows, sup) SL
+        cta_gemm(
+            Mrows, nS, nS, [&](int i, int k) { return g(fin ? i : a.act[i], a.sup[k]); }, ldSL,
+            [&](int i, int j, zc v) { T[i + (size_t)j * Mrows] = v; }, sA, sB, false);
+        __syncthreads();
+        // sum_q T(r, q) conj(w1(c, sup(q)))
+        auto blkv = [&](int r, int c) {
+            zc acc{0, 0};
+            for (int q = 0; q < nS; q++) cfma_conj(acc, T[r + (size_t)q * Mrows], g(c, a.sup[q]));
+            return acc;
+        };
+        if (fin) {
+            for (int i = threadIdx.x; i < N; i += blockDim.x) a.dosd[(size_t)iw * N + i] = g(i, i).y;
+            for (int t = threadIdx.x; t < 4 * a.N_sites; t += blockDim.x) {
+                int s = t >> 2, e = t & 3, aa = e & 1, bb = e >> 1;
+                a.onsL[(size_t)iw * 4 * a.N_sites + t] = blkv(2 * s + aa, 2 * s + bb);
+            }
+            if (a.atomL) {
+                for (int at = 0; at < a.N_atoms; at++) {
+                    int lo = 2 * (a.atom_first[at] - 1), m = 2 * a.atom_norb[at];
+                    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+                        int aa = t % m, bb = t / m;
+                        a.atomL[(size_t)iw * a.atomL_ld + a.atom_off[at] + t] = blkv(lo + aa, lo + bb);
+                    }
+                }
+            }
+            // current integrand through the left lead (src/scf.f90:390-409)
+            const int nCL = a.nCL;
+            for (int t = threadIdx.x; t < nCL * nCL; t += blockDim.x) {
+                int k = t % nCL, aa = t / nCL;
+                int ck = a.cl[k], ca = a.cl[aa];
+                zc glc = blkv(ck, ca);
+                zc gka = g(ck, ca), gak = conj(g(ca, ck));
+                zc gg = glc + gka - gak;
+                Xs[t] = zc{(fL - 1.0) * glc.x - fL * gg.x, (fL - 1.0) * glc.y - fL * gg.y};
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                zc tu{0, 0}, td{0, 0};
+                for (int aa = 0; aa < nCL; aa++) {
+                    zc mc{0, 0};
+                    for (int k = 0; k < nCL; k++) cfma(mc, a.GamLcl[aa + (size_t)k * nCL], Xs[k + (size_t)aa * nCL]);
+                    mc = zc{-mc.y, mc.x};
+                    if ((a.cl[aa] & 1) == 0) tu = tu + mc;  // 0-based even = spin up
+                    else td = td + mc;
+                }
+                a.trU[iw] = tu.x / (2.0 * PI);
+                a.trD[iw] = td.x / (2.0 * PI);
+            }
+        } else {
+            for (int k = threadIdx.x; k < a.nA; k += blockDim.x) {
+                int ak = a.act[k];
+                a.gRd[(size_t)iw * a.nA + k] = g(ak, ak);
+                a.gLd[(size_t)iw * a.nA + k] = blkv(k, ak);
+            }
+            for (int t = threadIdx.x; t < 4 * a.N_sites; t += blockDim.x) {
+                int s = t >> 2, e = t & 3, aa = e & 1, bb = e >> 1;
+                if (!a.site_int[s]) continue;
+                int lo = 2 * s, p1 = a.pos[lo];
+                a.onsL[(size_t)iw * 4 * a.N_sites + t] = blkv(p1 + aa, lo + bb);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Reductions over energies: out[c] = sum_r A[r*ld + c], deterministic.
+// ---------------------------------------------------------------------------------
+template <typename V>
+__global__ void colsum(const V *__restrict__ A, int64_t ld, int ncols, int64_t nrows, V *__restrict__ out) {
+    __shared__ V part[8][32];
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31), lane = threadIdx.x >> 5;
+    V acc{};
+    if (c < ncols)
+        for (int64_t r = lane; r < nrows; r += 8) {
+            V v = A[r * ld + c];
+            acc = acc + v;
+        }
+    part[lane][threadIdx.x & 31] = acc;
+    __syncthreads();
+    if (lane == 0 && c < ncols) {
+        V s = part[0][threadIdx.x];
+        for (int l = 1; l < 8; l++) s = s + part[l][threadIdx.x];
+        out[c] = s;
+    }
+}
+
+int sum_over_energies(qs_handle *h, const zc *d_A, int64_t ld, int ncols, int64_t nrows, zc *d_out) {
+    if (ncols <= 0) return 0;
+    colsum<zc><<<(ncols + 31) / 32, 256, 0, h->stream>>>(d_A, ld, ncols, nrows, d_out);
+    QS_CUDA(h, cudaGetLastError());
+    return 0;
+}
+int sum_over_energies_real(qs_handle *h, const double *d_A, int64_t ld, int ncols, int64_t nrows, double *d_out) {
+    if (ncols <= 0) return 0;
+    colsum<double><<<(ncols + 31) / 32, 256, 0, h->stream>>>(d_A, ld, ncols, nrows, d_out);
+    QS_CUDA(h, cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------------
+// pack_gf layout <-> device layout (per energy block of 3 nA^2 doubles)
+//   reference (common/linear_algebra.f90:155-191): Re G^r (row-major i,j) | Im G^r |
+//     Re G^< strict upper (row-major, j > i) | Im G^< upper (row-major, j >= i)
+// ---------------------------------------------------------------------------------
+__global__ void ref_dl_perm(int nA, int64_t Nw, const double *__restrict__ src, double *__restrict__ dst, int to_dl) {
+    const int64_t nblk = 3 * (int64_t)nA * nA;
+    const int nfull = nA * nA, nsu = (nfull - nA) / 2;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < Nw * nblk; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t w = t / nblk;
+        int e = (int)(t - w * nblk);
+        // e indexes the reference block; compute its device position
+        int64_t dpos;
+        if (e < 2 * nfull) {
+            int part = e / nfull, r = e % nfull;  // r = i*nA + j
+            int i = r / nA, j = r % nA;
+            dpos = 2 * ((int64_t)i + (int64_t)j * nA) + part;
+        } else if (e < 2 * nfull + nsu) {
+            int r = e - 2 * nfull;  // r-th strict-upper element in row-major order
+            // row i holds nA-1-i elements
+            int i = 0, acc = 0;
+            while (acc + (nA - 1 - i) <= r) { acc += nA - 1 - i; i++; }
+            int j = i + 1 + (r - acc);
+            dpos = 2 * (int64_t)nfull + 2 * ((int64_t)j * (j - 1) / 2 + i);
+        } else {
+            int r = e - 2 * nfull - nsu;  // r-th upper element (j >= i), row-major
+            int i = 0, acc = 0;
+            while (acc + (nA - i) <= r) { acc += nA - i; i++; }
+            int j = i + (r - acc);
+            if (i == j) dpos = 2 * (int64_t)nfull + (int64_t)nA * (nA - 1) + i;
+            else dpos = 2 * (int64_t)nfull + 2 * ((int64_t)j * (j - 1) / 2 + i) + 1;
+        }
+        if (to_dl) dst[w * nblk + dpos] = src[t];
+        else dst[t] = src[w * nblk + dpos];
+    }
+}
+
+int convert_ref_to_dl(cudaStream_t st, int nA, int64_t Nw, const double *ref, double *dl) {
+    ref_dl_perm<<<1184, 256, 0, st>>>(nA, Nw, ref, dl, 1);
+    return (int)cudaGetLastError();
+}
+int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, double *ref) {
+    ref_dl_perm<<<1184, 256, 0, st>>>(nA, Nw, dl, ref, 0);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------------
+static int dyson_threads(int N) { return N <= 128 ? (N <= 64 ? 256 : 512) : 512; }
+static size_t dyson_smem(int N) { return sizeof(zc) * (size_t)N * N; }
+static bool dyson_fits(int N) { return dyson_fits_smem(N); }
+
+static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
+    const int N = a.N;
+    int thr = dyson_threads(N);
+    size_t sm = 0;
+    if (dyson_fits(N)) {
+        sm = dyson_smem(N);
+        QS_CUDA(h, cudaFuncSetAttribute(dyson_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        a.ws = nullptr;
+    } else {
+        nblocks = std::min<int>(nblocks, (int)h->ws_slots);
+        a.ws = h->d_Gws;
+    }
+    dyson_gj<<<nblocks, thr, sm, h->stream>>>(a);
+    QS_CUDA(h, cudaGetLastError());
+    return 0;
+}
+
+int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, zc *d_ws, int ws_slots) {
+    DysonArgs a{};
+    a.N = N;
+    a.iw0 = 0;
+    a.iw1 = batch;
+    a.Ain = d_A;
+    a.out_mode = 1;
+    a.Gout = d_A;
+    a.info = d_info;
+    a.info_each = d_info + 1;
+    int thr = dyson_threads(N);
+    int nb = std::min(batch, 148 * 8);
+    size_t sm = 0;
+    if (dyson_fits(N)) {
+        sm = dyson_smem(N);
+        cudaError_t e = cudaFuncSetAttribute(dyson_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return -(int)e;
+    } else {
+        a.ws = d_ws;
+        nb = std::min(nb, ws_slots);
+    }
+    dyson_gj<<<nb, thr, sm, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : -(int)e;
+}
+
+// sweep(mode) over all energies (src/scf.f90:280-290).
+//   M_INIT2 / M_SCF2: output into d_out (SCF vector, DL); M_SCF2 subtracts d_x.
+//   M_SCF1 / M_FINAL: per-energy arrays of the handle.
+int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x) {
+    const int N = h->Norb, nA = h->nA, n = h->n;
+    DysonArgs a{};
+    a.N = N;
+    a.nA = nA;
+    a.Hemb = h->d_Hemb;
+    a.Sig1 = h->d_Sig1;
+    a.SigR = h->d_SigR;
+    a.pos = h->d_pos;
+    a.act = h->d_act;
+    a.omega = h->d_omega;
+    a.use_sigma = use_sigma;
+    a.order2 = (h->order == 2);
+    a.info = h->d_info;
+    int rc;
+    if (mode == M_INIT2 || mode == M_SCF2) {
+        a.iw0 = 0;
+        a.iw1 = n;
+        a.out_mode = 0;
+        a.Gout = h->d_G;
+        if ((rc = launch_dyson(h, a, std::min(n, 148 * 16)))) return rc;
+        KeldyshArgs k{};
+        k.nA = nA;
+        k.n = n;
+        k.nblk = h->nblk;
+        k.G = h->d_G;
+        k.SigL = (use_sigma && h->order == 2) ? h->d_SigL : nullptr;
+        k.GamLs = h->d_GamLs;
+        k.GamRs = h->d_GamRs;
+        k.omega = h->d_omega;
+        k.V = V;
+        k.mu = h->mu;
+        k.beta = h->beta;
+        k.out = d_out;
+        k.xsub = (mode == M_SCF2) ? d_x : nullptr;
+        k.gRd = h->d_gRd;
+        k.gLd = h->d_gLd;
+        k.Tws = h->d_T;
+        int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
+        keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
+        QS_CUDA(h, cudaGetLastError());
+        return 0;
+    }
+    // chunked full inversion + per-energy outputs
+    const int Mrows = (mode == M_FINAL) ? N : nA;
+    for (int iw0 = 0; iw0 < n; iw0 += (int)h->G_chunk) {
+        int iw1 = std::min(n, iw0 + (int)h->G_chunk);
+        a.iw0 = iw0;
+        a.iw1 = iw1;
+        a.out_mode = 1;
+        a.Gout = h->d_G;
+        if ((rc = launch_dyson(h, a, std::min(iw1 - iw0, 148 * 16)))) return rc;
+        FinalArgs f{};
+        f.N = N;
+        f.nS = h->nS;
+        f.nA = nA;
+        f.nCL = h->nCL;
+        f.N_sites = h->N_sites;
+        f.N_atoms = h->N_atoms;
+        f.iw0 = iw0;
+        f.iw1 = iw1;
+        f.mode = mode;
+        f.G = h->d_G;
+        f.sup = h->d_sup;
+        f.act = h->d_act;
+        f.pos = h->d_pos;
+        f.cl = h->d_cl;
+        f.site_int = h->d_site_int;
+        f.atom_first = h->d_atom_first;
+        f.atom_norb = h->d_atom_norb;
+        f.atom_off = h->d_atom_off;
+        f.GamLs = h->d_GamLs;
+        f.GamRs = h->d_GamRs;
+        f.GamLcl = h->d_GamLcl;
+        f.SigL = (use_sigma && h->order == 2) ? h->d_SigL : nullptr;
+        f.omega = h->d_omega;
+        f.V = V;
+        f.mu = h->mu;
+        f.beta = h->beta;
+        f.Tws = h->d_T;
+        f.dosd = h->d_dosd;
+        f.trU = h->d_trU;
+        f.trD = h->d_trD;
+        f.onsL = h->d_onsL;
+        f.atomL = h->has_atomL ? h->d_atomL : nullptr;
+        f.atomL_ld = h->has_atomL ? h->atom_off.back() : 0;
+        f.gRd = h->d_gRd;
+        f.gLd = h->d_gLd;
+        size_t per = (size_t)Mrows * h->nS;
+        int nb = (int)std::min<size_t>(std::min<size_t>(h->T_bytes / (sizeof(zc) * std::max<size_t>(per, 1)), 148 * 8),
+                                       (size_t)(iw1 - iw0));
+        nb = std::max(nb, 1);
+        final_outputs<<<nb, 256, 0, h->stream>>>(f);
+        QS_CUDA(h, cudaGetLastError());
+    }
+    return 0;
+}
+
+}  // namespace qs

@@ -1,0 +1,104 @@
+"""Parity of each CUDA step with the oracle on the same inputs (FP64; tolerances stated
+per test). Every call goes through the C ABI of libqsb200.so."""
+import os
+
+import numpy as np
+import pytest
+
+import golden_runner as g
+import oracle_lib
+import quichotte_b200 as qb
+
+pytestmark = pytest.mark.gpu
+CASES = os.path.join(g.GOLDEN, "cases")
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("N", [1, 2, 5, 8, 16, 33, 64, 100, 120, 121, 200])
+def test_invert_batched_matches_numpy(N):
+    rng = np.random.default_rng(N)
+    batch = 37
+    A = rng.standard_normal((batch, N, N)) + 1j * rng.standard_normal((batch, N, N)) + 3 * np.sqrt(N) * np.eye(N)
+    inv, info = qb.invert_batched(A)
+    assert not info.any()
+    assert rel(inv, np.linalg.inv(A)) < 1e-13  # FP64, well-conditioned
+
+
+def test_invert_batched_flags_singular_matrix():
+    A = np.tile(np.eye(6, dtype=np.complex128), (4, 1, 1))
+    A[2, 3, :] = 0.0  # matrix 2 has a zero row
+    inv, info = qb.invert_batched(A)
+    assert info[2] != 0 and not info[[0, 1, 3]].any()
+    assert np.allclose(inv[0], np.eye(6))
+
+
+def test_pack_unpack_bit_exact_against_oracle():
+    rng = np.random.default_rng(2)
+    nb, Nw = 6, 11
+    Gr = np.asfortranarray(rng.standard_normal((nb, nb, Nw)) + 1j * rng.standard_normal((nb, nb, Nw)))
+    A = rng.standard_normal((nb, nb, Nw)) + 1j * rng.standard_normal((nb, nb, Nw))
+    Gl = np.asfortranarray(A - np.conj(A.transpose(1, 0, 2)))
+    x_gpu = qb.pack_gf(Gr, Gl)
+    x_ora = qb.pack_gf(Gr, Gl, lib=oracle_lib.lib(), prefix="qso_")
+    assert np.array_equal(x_gpu, x_ora)
+    R, L = qb.unpack_gf(x_gpu, nb, Nw)
+    R2, L2 = qb.unpack_gf(x_gpu, nb, Nw, lib=oracle_lib.lib(), prefix="qso_")
+    assert np.array_equal(R, R2) and np.array_equal(L, L2)
+
+
+ORDER2 = ["order2_second_order", "order2_lefthanded_siteU", "order2_dftb_blocks", "order2_dftb_hs"]
+
+
+def pair(case):
+    m = qb.Model.load(os.path.join(CASES, case))
+    return m, qb.Solver(m), oracle_lib.solver(m)
+
+
+@pytest.mark.parametrize("case", ORDER2)
+def test_initial_vector_matches_oracle(case):
+    m, gs, os_ = pair(case)
+    assert gs.n_vec == os_.n_vec and gs.nA == os_.nA and gs.Nf == os_.Nf
+    xg, xo = gs.initial_vector(m.V), os_.initial_vector(m.V)
+    assert rel(xg, xo) < 1e-12
+
+
+@pytest.mark.parametrize("case", ORDER2)
+def test_self_energies_match_oracle(case):
+    m, gs, os_ = pair(case)
+    x = os_.initial_vector(m.V)
+    x = x + 1e-3 * np.random.default_rng(0).standard_normal(x.size)
+    SRg, SLg, S1g = gs.self_energies(x)
+    SRo, SLo, S1o = os_.self_energies(x)
+    assert rel(SRg, SRo) < 1e-12
+    assert rel(SLg, SLo) < 1e-12
+    assert np.max(np.abs(S1g - S1o)) < 1e-13
+
+
+@pytest.mark.parametrize("case", ORDER2 + ["order1_hartree_fock", "order1_custom_template"])
+def test_residual_matches_oracle(case):
+    m, gs, os_ = pair(case)
+    x = os_.initial_vector(m.V)
+    Fg, ag = gs.residual(m.V, x)
+    Fo, ao = os_.residual(m.V, x)
+    assert ag == ao == False
+    assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_device_broyden_matches_oracle_broyden(single):
+    rng = np.random.default_rng(7)
+    n = 300
+    A = 0.5 * rng.standard_normal((n, n)) / np.sqrt(n)
+    b = rng.standard_normal(n)
+    res = lambda x: (np.tanh(A @ x) + b - x, False)
+    kw = dict(alpha_mix=0.2, nhist=8, maxscf=100, tolf=1e-11, single_history=single)
+    xg, cg, ng, fg, sg = qb.broyden_solve(res, np.zeros(n), **kw)
+    xo, co, no, fo, so = qb.broyden_solve(res, np.zeros(n), lib=oracle_lib.lib(), prefix="qso_", **kw)
+    assert cg and co and ng == no
+    assert np.max(np.abs(xg - xo)) < 1e-10
+    for a, b_ in zip(sg, so):
+        assert a[0] == b_[0] and a[3] == b_[3]
+        assert abs(a[1] - b_[1]) <= 1e-9 * max(b_[1], 1e-12) + 1e-14

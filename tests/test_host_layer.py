@@ -1,0 +1,75 @@
+"""The host layer (input.dat, models, grid, output format) against the reference's
+golden files (CPU only)."""
+import os
+
+import numpy as np
+import pytest
+
+import golden_runner as g
+import quichotte_b200 as qb
+
+CASES = os.path.join(g.GOLDEN, "cases")
+
+
+def test_list_directed_format_reproduces_golden_lines():
+    import ctypes
+    buf = ctypes.create_string_buffer(64)
+
+    def fmt(x):
+        qb._host.qsh_fmt_real(x, buf)
+        return buf.value.decode()
+
+    for case in ("order2_second_order", "order2_dftb_hs", "order0_dftb_blocks"):
+        for name in os.listdir(os.path.join(CASES, case, "reference")):
+            if name == "hamiltonian_matrix.dat":
+                continue
+            for line in open(os.path.join(CASES, case, "reference", name)):
+                line = line.rstrip("\n")
+                toks = line.split()
+                out = ""
+                for i, t in enumerate(toks):
+                    if "." in t or "E" in t:
+                        out += fmt(float(t))
+                    else:
+                        out += f" {int(t):11d}"
+                assert out == line
+
+
+@pytest.mark.parametrize("case", ["error_N_sites_mismatch", "error_unknown_hamiltonian", "error_dftb_lead_overlap",
+                                  "error_dftb_hs_no_lmax"])
+def test_bad_inputs_are_rejected(case):
+    with pytest.raises(ValueError):
+        qb.Model.load(os.path.join(CASES, case))
+
+
+def test_legacy_input_name_and_aliases():
+    m = qb.Model.load(os.path.join(CASES, "legacy_inputSOC"))
+    assert m.order == 1 and m.alpha_mix == 0.5 and m.Norb == 8
+    assert np.all(m.U_site[::2] == 0.8)
+
+
+def test_dftb_hs_hamiltonian_matches_golden():
+    m = qb.Model.load(os.path.join(CASES, "order2_dftb_hs"))
+    ref = np.loadtxt(os.path.join(CASES, "order2_dftb_hs", "reference", "hamiltonian_matrix.dat"))
+    H = np.zeros_like(m.H)
+    for i, j, re, im in ref:
+        H[int(i) - 1, int(j) - 1] = re + 1j * im
+    assert np.max(np.abs(H - m.H)) < 1e-12
+    assert np.allclose(m.H, m.H.conj().T, atol=0)
+
+
+def test_helix_grid_and_hermiticity():
+    m = qb.Model.load(os.path.join(CASES, "order2_second_order"))
+    ev = np.linalg.eigvalsh(m.H)
+    w_init = ev[0] - 1.0
+    n = int((ev[-1] + 1.0 - w_init) / m.delta)
+    assert m.n_omega == n == 329
+    assert np.allclose(m.omega, w_init + m.delta * np.arange(1, n + 1), atol=1e-12)
+    assert np.allclose(m.H, m.H.conj().T, atol=0)
+    # leads on site 1 (spin-dependent) and the last site
+    assert m.GammaL[0, 0] == 1.5 and m.GammaL[1, 1] == 1.0 and m.GammaR[-1, -1] == 1.0
+
+
+def test_site_dependent_U():
+    m = qb.Model.load(os.path.join(CASES, "order2_lefthanded_siteU"))
+    assert list(m.U_site[::2]) == [0.8, 0.6, 0.6, 0.8] and not m.U_site[1::2].any()
