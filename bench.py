@@ -1,0 +1,296 @@
+"""Benchmark: converged IV points per second of QUICHOTTE's order-2 SCF on B200.
+
+Workload (one "step" = one IV point: solve_scf at the next voltage of the sweep, with
+continuation from the previous one, then Current and the observables):
+  helix of 10 sites/turn x 6 turns (60 sites, 120x120 complex H), E_CC = 0, t = 1.0 eV,
+  SOC lambda = 0.01 eV, radius 0.7 nm, pitch 0.34 nm/turn, hand = +1, wide-band leads
+  Gamma_L = Gamma_R = 0.5 eV on the first and last site, U = 1.0 eV on every site,
+  2nd order, T = 300 K, mu = 0, 16384 energies on [-12, 12] eV, V from -1 to 1 V in
+  steps of 0.05 V (41 voltages), Broyden: reference defaults (alpha_mix 0.5, 16-column
+  single-precision history, tolf 1e-6). Synthetic input (the model is analytic).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (launched with torch.distributed.run): replicas. Rank r solves its own contiguous
+block of the voltage sweep; no data-path collective. value = all IV points / max over
+ranks of the device time. The reference arm (--impl reference) times the CPU oracle
+(a restatement of the reference's Fortran path) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "quichotte-and-sancho_b200"))
+
+N_IONS, N_TURNS = 10, 6
+PITCH, RADIUS = 0.34, 0.7
+N_OMEGA, W_LO, W_HI = 16384, -12.0, 12.0
+VOLTS = [round(-1.0 + 0.05 * k, 10) for k in range(41)]
+
+
+def model_cfg1(qb, n_omega=N_OMEGA):
+    """Helix model with its grid exactly on [W_LO, W_HI] with n_omega points
+    (omega_i = w_init + i*delta, i = 1..n; w_init = Ev_min - dw, n = int((w_fin-w_init)/delta))."""
+    hel_length = PITCH * N_TURNS * (N_IONS - 1) / N_IONS  # dz = pitch / N_ions
+    args = dict(N_ions=N_IONS, N_turns=N_TURNS, hel_length=hel_length, hel_radius=RADIUS, hand=1.0, E_CC=0.0,
+                t_hop=1.0, lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0)
+    probe = qb.Model.helix(dw=1.0, up=1.0, delta=0.1, **args)
+    ev = np.linalg.eigvalsh(probe.H)
+    delta = (W_HI - W_LO) / n_omega
+    dw = ev[0] - W_LO  # w_init = W_LO, omega_n = W_LO + n delta = W_HI
+    up = W_HI - ev[-1]
+    m = qb.Model.helix(dw=dw, up=up, delta=delta, **args)
+    if m.n_omega == n_omega - 1:  # int() truncation of (w_fin - w_init)/delta (src/quichotte.f90:246)
+        up += 0.5 * delta
+        m = qb.Model.helix(dw=dw, up=up, delta=delta, **args)
+    assert m.n_omega == n_omega, m.n_omega
+    m.alpha_mix, m.nhist, m.tolf, m.maxscf, m.single_history = 0.5, 16, 1e-6, 300, True
+    return m
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.samples, self.index = [], index
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for k, nm in enumerate(names):
+                    if s[4 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# SCF steps per IV point of this workload, measured on B200 (both arms run the same
+# Broyden algorithm, so the oracle takes the same number of steps up to rounding)
+STEPS_PER_POINT = 25.5
+
+
+def cpu_baseline_sample(n_sample=4096, steps_per_point=STEPS_PER_POINT, threads=None):
+    """The CPU oracle on a bounded sample of the workload: one SCF step (scf_residual2:
+    Sigma2 by FFT + the Dyson/Keldysh sweep) of the same helix on the same energy window
+    with n_sample energies, scaled linearly to the 16384-energy grid and multiplied by the
+    SCF steps of one IV point. The Broyden update is left out (in the CPU's favour)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    import quichotte_b200 as qb
+    m = model_cfg1(qb, n_sample)
+    s = oracle_lib.solver(m, nhist=0)
+    x = s.initial_vector(VOLTS[0])
+    t0 = time.perf_counter()
+    F, ab = s.residual(VOLTS[0], x)
+    dt = time.perf_counter() - t0
+    s.close()
+    scale = N_OMEGA / n_sample
+    per_point = dt * scale * steps_per_point
+    return {"value": 1.0 / per_point, "unit": "IV points/s", "cores": threads or os.cpu_count(), "kind": "port",
+            "sample": f"CPU oracle (OpenMP, OpenBLAS zgetrf/zgetri, own FFT), one scf_residual2 of the same helix "
+                      f"on {n_sample} energies over [-12,12] eV: {dt:.2f} s; x{scale:g} to 16384 energies and "
+                      f"x{steps_per_point:g} SCF steps per IV point; Broyden update not counted"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle (a restatement of the reference's CPU path: OpenMP
+    over energies, LAPACK zgetrf/zgetri from OpenBLAS, its own FFT) on the host cores."""
+    if rank != 0:
+        return 0
+    nthr = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(nthr))
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cb = cpu_baseline_sample(args.ref_sample, threads=nthr)
+        if k >= args.warmup:
+            times.append(1.0 / cb["value"])
+    t = sum(times)
+    v = args.steps / t
+    line = {"metric": "converged IV points/s", "value": v, "unit": "IV points/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "helix 10x6 (120x120), 16384 energies on [-12,12] eV, order 2, U=1.0 eV, "
+                                   "V sweep -1..1 V step 0.05"},
+            "cpu_baseline": {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port", "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "IV points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=4096)
+    ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
+    ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import quichotte_b200 as qb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    m = model_cfg1(qb, args.n_omega)
+    solver = qb.Solver(m, device=local, alpha_mix=0.5, nhist=args.nhist, tolf=1e-6, maxscf=300, single_history=1)
+    # this rank's block of the voltage sweep
+    per = (len(VOLTS) + world - 1) // world
+    block = VOLTS[rank * per:(rank + 1) * per] or VOLTS[-1:]
+    seq = [block[k % len(block)] for k in range(args.warmup + args.steps)]
+    fresh = [k == 0 or (k % len(block) == 0) for k in range(len(seq))]
+
+    obs_bytes = 8 * (2 * m.Norb * m.Norb + m.Norb * m.n_omega + 2 * m.n_omega)
+    n_conv, iters = 0, []
+    prev_ok = False
+    for k in range(args.warmup):
+        # continuation as the reference's sweep: fresh after an unconverged voltage
+        r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
+        prev_ok = r["converged"]
+        solver.current(seq[k])
+        solver.observables()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    solver.profile(True)
+    l0 = qb.kernel_launches()
+    dev_s, wall0 = 0.0, time.perf_counter()
+    currents = []
+    for k in range(args.warmup, args.warmup + args.steps):
+        r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
+        prev_ok = r["converged"]
+        dev_s += r["seconds"]
+        n_conv += int(r["converged"])
+        iters.append(r["n_iter"])
+        currents.append(solver.current(seq[k]))
+        solver.observables()  # G_less_obs, dosd, trU, trD back to host buffers
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    launches = qb.kernel_launches() - l0
+    prof = solver.profile(False)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([dev_s, wall, float(n_conv)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
+        tc = t[2:].clone()
+        dist.all_reduce(tc, op=dist.ReduceOp.SUM)
+        dev_s, wall, n_conv = float(t[0]), float(t[1]), int(tc[0])
+        dist.barrier()
+    if rank == 0:
+        points = args.steps * world
+        peaks, src = measured_peaks()
+        # roofline of the dominant kernel (largest device time): algorithmic work per launch
+        N, nA, n = m.Norb, solver.nA, m.n_omega
+        fam, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+        nY, Nf, nvec = nA * nA + nA * (nA + 1) // 2, solver.Nf, solver.n_vec
+        nh = args.nhist
+        work = {  # algorithmic FLOPs (FP64 compute-bound kernels) or bytes (HBM-bound) per launch
+            "dyson_gj": ("fp64", n * 8.0 * N ** 3),                       # G^r: N^3 complex MACs per energy
+            "keldysh_scf2": ("fp64", n * 16.0 * nA ** 3),                 # G^< = G SL G^a: 2 nA^3 complex MACs
+            "sig2_fwdA": ("hbm", nvec * 8.0 + nY * Nf * 16.0),            # read packed G, write Y
+            "sig2_mid": ("hbm", (nY + 2.0 * nA * nA) * Nf * 16.0),         # read Y, write V
+            "sig2_invC": ("hbm", 2.0 * nA * nA * Nf * 16.0 + 2.0 * nA * nA * n * 16.0),  # read V, write Sigma
+            "broyden": ("hbm", nvec * (64.0 + 12.0 * nh) / 3.0),          # per iteration / 3 launches
+        }
+        roof = None
+        if fam in work and cnt:
+            kind, per_launch = work[fam]
+            t = ms / cnt * 1e-3
+            if kind == "fp64":
+                achieved, peak, unit = per_launch / t / 1e12, 37.0, "TFLOP/s"
+                src_note = "nominal B200 FP64 37 TFLOP/s (MEASURED_PEAKS.json has no FP64 figure)"
+            else:
+                achieved, peak, unit = per_launch / t / 1e9, peaks.get("hbm_gbs", 6650.0), "GB/s"
+                src_note = f"hbm_gbs of MEASURED_PEAKS.json ({src})"
+            roof = {"kernel": fam, "bound": kind, "achieved": achieved, "peak": peak, "unit": unit,
+                    "frac": achieved / peak, "traffic": None, "peak_source": src_note,
+                    "per_launch_work": per_launch, "launches": cnt, "avg_launch_ms": ms / cnt}
+        line = {
+            "metric": "converged IV points/s", "value": n_conv / dev_s if dev_s > 0 else 0.0,
+            "unit": "IV points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"helix 10x6 (120x120 complex), {n} energies on [-12,12] eV, order 2, U=1.0 eV, "
+                                   "V sweep -1..1 V step 0.05 with continuation", "precision": "fp64", "nhist": args.nhist,
+                       "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 (no flush needed)",
+                       "scf_steps_per_point": iters, "converged_points": n_conv},
+            "e2e": {"value": n_conv / wall if wall > 0 else 0.0, "unit": "IV points/s", "h2d_bytes_per_step": 8,
+                    "d2h_bytes_per_step": obs_bytes},
+            "gpu_launches": launches,
+            "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
+            "roofline": roof,
+            "clocks": clk,
+            "currents_A": [list(c) for c in currents],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(args.ref_sample)
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

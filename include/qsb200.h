@@ -123,6 +123,18 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
                           int nhist, int maxscf, double tolf, int single_history, int *converged,
                           int *n_iter, double *fmax, qs_scf_step *log, int log_cap);
 
+/* ---- instrumentation (no counterpart in the reference, whose only timer is the
+ * wall clock of src/quichotte.f90:50-58) ---- */
+
+/* Number of kernels this library has launched in the process so far. */
+int64_t qs_kernel_launches(void);
+
+/* Per-kernel-family device time measured with CUDA events on the solver's stream.
+ * enable = 1 starts recording, 0 stops, -1 only reads and resets. Fills ms[f] and
+ * launches[f] for f < nfam (families: 0 Dyson, 1 Keldysh, 2-4 Sigma2 FFT kernels A/B/C,
+ * 5 final-sweep outputs, 6 Broyden, 7 reductions, 8 other). Returns the family count. */
+int qs_profile(qs_handle *h, int enable, double *ms, int64_t *launches, int nfam);
+
 #ifdef __cplusplus
 }
 #endif

@@ -232,7 +232,10 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
         }
         // max|F|, ||F||, ||F - Fold||
         const bool want_dn = its > 1 && nhist > 0;
+        int pi = prof_begin(h, K_BROYDEN);
         vec_norms<<<nb, RED_THREADS, 0, st>>>(d_F, want_dn ? d_Fold : nullptr, n, part);
+        prof_end(h, pi);
+        count_launch();
         part_reduce<<<1, 32, 0, st>>>(part, nb, 3, 3, 1, fin);
         QS_CUDA(h, cudaGetLastError());
         QS_CUDA(h, cudaMemcpyAsync(hv.data(), fin, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -249,12 +252,15 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
         int slot = want_dn ? nstored % nhist : 0;
         int nh_new = store ? std::min(nstored + 1, nhist) : std::min(nstored, nhist);
         if (nh_new > 0 || store) {
+            int pj = prof_begin(h, K_BROYDEN);
             if (sp)
                 launch_hist<float>(nb, st, d_F, d_Fold, d_x, d_xold, n, store ? fnorm : 1.0, alpha_mix, (float *)d_hdF,
                                    (float *)d_hU, slot, nh_new, store, part);
             else
                 launch_hist<double>(nb, st, d_F, d_Fold, d_x, d_xold, n, store ? fnorm : 1.0, alpha_mix, (double *)d_hdF,
                                     (double *)d_hU, slot, nh_new, store, part);
+            prof_end(h, pj);
+            count_launch();
             part_reduce<<<1, 2 * MAXH, 0, st>>>(part, nb, 2 * MAXH, 2 * nh_new, 0, fin);
             QS_CUDA(h, cudaGetLastError());
             QS_CUDA(h, cudaMemcpyAsync(hv.data(), fin, 2 * nh_new * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -284,10 +290,12 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
             }
         }
         // x_new into the xold buffer, then rotate: xold <- x, x <- x_new, Fold <- F
+        int pk = prof_begin(h, K_BROYDEN);
         if (sp)
             x_update<float><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const float *)d_hU, gam, nh, alpha_mix, n, d_xold);
         else
             x_update<double><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const double *)d_hU, gam, nh, alpha_mix, n, d_xold);
+        prof_end(h, pk);
         QS_CUDA(h, cudaGetLastError());
         std::swap(d_x, d_xold);
         std::swap(d_F, d_Fold);

@@ -98,7 +98,18 @@ struct DeviceBuf {
 
 }  // namespace qs
 
+namespace qs {
+// kernel families timed by the optional profiler (qs_profile)
+enum KernelFamily { K_DYSON = 0, K_KELDYSH, K_SIG2A, K_SIG2B, K_SIG2C, K_FINAL, K_BROYDEN, K_REDUCE, K_OTHER, K_NFAM };
+}  // namespace qs
+
 struct qs_handle {
+    // optional per-launch CUDA-event timing on the solver stream
+    bool prof_on = false;
+    std::vector<cudaEvent_t> prof_ev;           // pool, 2 per timed launch
+    std::vector<int> prof_fam;                  // family of launch i (events 2i, 2i+1)
+    double prof_ms[qs::K_NFAM] = {0};
+    int64_t prof_count[qs::K_NFAM] = {0};
     // problem (host copies)
     int Norb = 0, N_sites = 0, N_atoms = 0, order = 0, n = 0, device = 0, precision = 0;
     double mu = 0, beta = 0, delta = 0, alpha_mix = 0.5, tolf = 1e-6, tolf_order1 = 1e-8;
@@ -171,6 +182,12 @@ namespace qs {
     } while (0)
 
 int dalloc(qs_handle *h, void **p, size_t bytes);
+
+// every kernel launch of the library is counted (qs_kernel_launches)
+void count_launch();
+// bracket a launch with events when profiling is on: idx = prof_begin(...); launch; prof_end(h, idx)
+int prof_begin(qs_handle *h, int fam);
+void prof_end(qs_handle *h, int idx);
 
 // launchers (implemented in the .cu files)
 int sigma2_setup(qs_handle *h);

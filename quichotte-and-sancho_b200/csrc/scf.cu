@@ -18,9 +18,34 @@
 
 #include "qs_common.cuh"
 
+#include <atomic>
+
 namespace qs {
 
 size_t broyden_red_len();
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int prof_begin(qs_handle *h, int fam) {
+    count_launch();
+    if (!h->prof_on) return -1;
+    size_t i = h->prof_fam.size();
+    if (2 * i + 2 > h->prof_ev.size()) {
+        for (int k = 0; k < 64; k++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            h->prof_ev.push_back(e);
+        }
+    }
+    h->prof_fam.push_back(fam);
+    cudaEventRecord(h->prof_ev[2 * i], h->stream);
+    return (int)i;
+}
+void prof_end(qs_handle *h, int idx) {
+    if (idx < 0) return;
+    cudaEventRecord(h->prof_ev[2 * idx + 1], h->stream);
+}
 
 int dalloc(qs_handle *h, void **p, size_t bytes) {
     *p = nullptr;
@@ -90,8 +115,10 @@ __global__ void glt0_sigma1(const double *__restrict__ x, int64_t nblk, int n, i
 }
 
 int equal_time_lesser_sigma1(qs_handle *h, const double *d_x) {
+    int pi = prof_begin(h, K_REDUCE);
     glt0_sigma1<<<h->nAs, 256, 0, h->stream>>>(d_x, h->nblk, h->n, h->nA, h->Norb, h->d_act, h->d_U,
                                                 h->delta / (2.0 * PI), h->d_Glt0, h->d_Sig1);
+    prof_end(h, pi);
     QS_CUDA(h, cudaGetLastError());
     return 0;
 }
@@ -585,6 +612,7 @@ int qs_create(const qs_problem *p, qs_handle **out) {
 void qs_destroy(qs_handle *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     for (void *p : h->allocs) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -593,6 +621,32 @@ void qs_destroy(qs_handle *h) {
 }
 
 const char *qs_last_error(const qs_handle *h) { return h ? h->err.c_str() : "no handle"; }
+
+int64_t qs_kernel_launches(void) { return g_launches.load(); }
+
+int qs_profile(qs_handle *h, int enable, double *ms, int64_t *launches, int nfam) {
+    QS_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < h->prof_fam.size(); i++) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]) == cudaSuccess) {
+            h->prof_ms[h->prof_fam[i]] += t;
+            h->prof_count[h->prof_fam[i]] += 1;
+        }
+    }
+    h->prof_fam.clear();
+    for (int f = 0; f < K_NFAM && f < nfam; f++) {
+        if (ms) ms[f] = h->prof_ms[f];
+        if (launches) launches[f] = h->prof_count[f];
+    }
+    if (enable < 0 || enable != (int)h->prof_on) {  // reset the totals when switching
+        for (int f = 0; f < K_NFAM; f++) {
+            h->prof_ms[f] = 0;
+            h->prof_count[f] = 0;
+        }
+    }
+    if (enable >= 0) h->prof_on = enable != 0;
+    return K_NFAM;
+}
 int64_t qs_vector_length(const qs_handle *h) { return h->n_vec; }
 int qs_active_states(const qs_handle *h) { return h->nA; }
 int qs_fft_length(const qs_handle *h) { return h->order == 2 ? h->fft.Nf : good_fft_size_h(2 * h->n - 1); }
@@ -864,6 +918,7 @@ int qs_pack_gf(int nb, int Nw, const double *Gr, const double *Gl, double *out) 
     cudaMalloc(&dO, sizeof(double) * blk * Nw);
     cudaMemcpy(dR, Gr, sizeof(zc) * nf * Nw, cudaMemcpyHostToDevice);
     cudaMemcpy(dL, Gl, sizeof(zc) * nf * Nw, cudaMemcpyHostToDevice);
+    count_launch();
     pack_ref<<<1184, 256>>>(nb, Nw, dR, dL, dO);
     cudaError_t e = cudaMemcpy(out, dO, sizeof(double) * blk * Nw, cudaMemcpyDeviceToHost);
     cudaFree(dR);
@@ -879,6 +934,7 @@ int qs_unpack_gf(int nb, int Nw, const double *in, double *Gr, double *Gl) {
     cudaMalloc(&dL, sizeof(zc) * nf * Nw);
     cudaMalloc(&dI, sizeof(double) * blk * Nw);
     cudaMemcpy(dI, in, sizeof(double) * blk * Nw, cudaMemcpyHostToDevice);
+    count_launch();
     unpack_ref<<<1184, 256>>>(nb, Nw, dI, dR, dL);
     cudaError_t e = cudaMemcpy(Gr, dR, sizeof(zc) * nf * Nw, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(Gl, dL, sizeof(zc) * nf * Nw, cudaMemcpyDeviceToHost);

@@ -362,7 +362,7 @@ int sigma2_setup(qs_handle *h) {
     }
     int rc;
     if ((rc = dalloc(h, (void **)&h->d_tw, sizeof(zc) * fp.Nf))) return rc;
-    QS_CUDA(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(zc) * fp.Nf, cudaMemcpyHostToDevice));
+    QS_CUDA(h, cudaMemcpyAsync(h->d_tw, tw.data(), sizeof(zc) * fp.Nf, cudaMemcpyHostToDevice, h->stream));
     // Y sequences: every G^r element, the upper triangle of G^<
     const int nfull = nA * nA;
     std::vector<int2> desc;
@@ -381,7 +381,7 @@ int sigma2_setup(qs_handle *h) {
     h->nY = desc.size();
     h->nV = (size_t)2 * nfull;
     if ((rc = dalloc(h, (void **)&h->d_ydesc, sizeof(int2) * desc.size()))) return rc;
-    QS_CUDA(h, cudaMemcpy(h->d_ydesc, desc.data(), sizeof(int2) * desc.size(), cudaMemcpyHostToDevice));
+    QS_CUDA(h, cudaMemcpyAsync(h->d_ydesc, desc.data(), sizeof(int2) * desc.size(), cudaMemcpyHostToDevice, h->stream));
     if ((rc = dalloc(h, (void **)&h->d_Y, sizeof(zc) * h->nY * fp.Nf))) return rc;
     if ((rc = dalloc(h, (void **)&h->d_V, sizeof(zc) * h->nV * fp.Nf))) return rc;
     if ((rc = dalloc(h, (void **)&h->d_SigR, sizeof(zc) * (size_t)nfull * n))) return rc;
@@ -400,9 +400,10 @@ int sigma2_setup(qs_handle *h) {
     double *dU;
     int2 *dP;
     if ((rc = dalloc(h, (void **)&dU, sizeof(double) * Upair.size()))) return rc;
-    QS_CUDA(h, cudaMemcpy(dU, Upair.data(), sizeof(double) * Upair.size(), cudaMemcpyHostToDevice));
+    QS_CUDA(h, cudaMemcpyAsync(dU, Upair.data(), sizeof(double) * Upair.size(), cudaMemcpyHostToDevice, h->stream));
     if ((rc = dalloc(h, (void **)&dP, sizeof(int2) * std::max<size_t>(pairs.size(), 1)))) return rc;
-    if (!pairs.empty()) QS_CUDA(h, cudaMemcpy(dP, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice));
+    if (!pairs.empty())
+        QS_CUDA(h, cudaMemcpyAsync(dP, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, h->stream));
     h->sig2_Upair = dU;
     h->sig2_pairs = dP;
     h->sig2_npairs = (int)pairs.size();
@@ -427,6 +428,9 @@ int sigma2_setup(qs_handle *h) {
     h->sig2_smem[0] = smA;
     h->sig2_smem[1] = smB;
     h->sig2_smem[2] = smC;
+    // every buffer is zeroed on h->stream by dalloc: the tables are copied on the same
+    // stream (after the zeroing) and the host staging vectors must outlive the copies
+    QS_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
 
@@ -434,17 +438,23 @@ int sigma2_compute(qs_handle *h, const double *d_x) {
     const FftPlan &fp = h->fft;
     const int nA = h->nA;
     dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
+    int pa = prof_begin(h, K_SIG2A);
     sig2_fwdA<double><<<gA, 256, h->sig2_smem[0], h->stream>>>(d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw,
                                                              h->d_Y, h->sig2_SA, h->sig2_GA);
+    prof_end(h, pa);
     QS_CUDA(h, cudaGetLastError());
     if (h->sig2_npairs > 0) {
         dim3 gB((unsigned)h->sig2_npairs, (unsigned)(fp.N1 / 2 + 1));
+        int pb = prof_begin(h, K_SIG2B);
         sig2_mid<double><<<gB, 256, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw);
+        prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
     dim3 gC((unsigned)(h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
+    int pc = prof_begin(h, K_SIG2C);
     sig2_invC<double><<<gC, 256, h->sig2_smem[2], h->stream>>>(h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n,
                                                              h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
+    prof_end(h, pc);
     QS_CUDA(h, cudaGetLastError());
     return 0;
 }

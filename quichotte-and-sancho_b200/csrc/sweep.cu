@@ -420,13 +420,17 @@ __global__ void colsum(const V *__restrict__ A, int64_t ld, int ncols, int64_t n
 
 int sum_over_energies(qs_handle *h, const zc *d_A, int64_t ld, int ncols, int64_t nrows, zc *d_out) {
     if (ncols <= 0) return 0;
+    int pi = prof_begin(h, K_REDUCE);
     colsum<zc><<<(ncols + 31) / 32, 256, 0, h->stream>>>(d_A, ld, ncols, nrows, d_out);
+    prof_end(h, pi);
     QS_CUDA(h, cudaGetLastError());
     return 0;
 }
 int sum_over_energies_real(qs_handle *h, const double *d_A, int64_t ld, int ncols, int64_t nrows, double *d_out) {
     if (ncols <= 0) return 0;
+    int pi = prof_begin(h, K_REDUCE);
     colsum<double><<<(ncols + 31) / 32, 256, 0, h->stream>>>(d_A, ld, ncols, nrows, d_out);
+    prof_end(h, pi);
     QS_CUDA(h, cudaGetLastError());
     return 0;
 }
@@ -469,10 +473,12 @@ __global__ void ref_dl_perm(int nA, int64_t Nw, const double *__restrict__ src, 
 }
 
 int convert_ref_to_dl(cudaStream_t st, int nA, int64_t Nw, const double *ref, double *dl) {
+    count_launch();
     ref_dl_perm<<<1184, 256, 0, st>>>(nA, Nw, ref, dl, 1);
     return (int)cudaGetLastError();
 }
 int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, double *ref) {
+    count_launch();
     ref_dl_perm<<<1184, 256, 0, st>>>(nA, Nw, dl, ref, 0);
     return (int)cudaGetLastError();
 }
@@ -496,7 +502,9 @@ static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
         nblocks = std::min<int>(nblocks, (int)h->ws_slots);
         a.ws = h->d_Gws;
     }
+    int pi = prof_begin(h, K_DYSON);
     dyson_gj<<<nblocks, thr, sm, h->stream>>>(a);
+    prof_end(h, pi);
     QS_CUDA(h, cudaGetLastError());
     return 0;
 }
@@ -522,6 +530,7 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
         a.ws = d_ws;
         nb = std::min(nb, ws_slots);
     }
+    count_launch();
     dyson_gj<<<nb, thr, sm, st>>>(a);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : -(int)e;
@@ -569,7 +578,9 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
         int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
+        int pi = prof_begin(h, K_KELDYSH);
         keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
+        prof_end(h, pi);
         QS_CUDA(h, cudaGetLastError());
         return 0;
     }
@@ -622,7 +633,9 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         int nb = (int)std::min<size_t>(std::min<size_t>(h->T_bytes / (sizeof(zc) * std::max<size_t>(per, 1)), 148 * 8),
                                        (size_t)(iw1 - iw0));
         nb = std::max(nb, 1);
+        int pi = prof_begin(h, K_FINAL);
         final_outputs<<<nb, 256, 0, h->stream>>>(f);
+        prof_end(h, pi);
         QS_CUDA(h, cudaGetLastError());
     }
     return 0;

@@ -127,11 +127,21 @@ def bind_solver(lib, prefix):
 
 
 bind_solver(_lib, "qs_")
+_lib.qs_kernel_launches.restype = ctypes.c_int64
+_lib.qs_profile.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+KERNEL_FAMILIES = ("dyson_gj", "keldysh_scf2", "sig2_fwdA", "sig2_mid", "sig2_invC", "final_outputs", "broyden",
+                   "reductions", "other")
+
+
+def kernel_launches():
+    """Kernels launched by libqsb200.so in this process so far."""
+    return int(_lib.qs_kernel_launches())
 
 # every entry point of include/qsb200.h (the loader test checks they are all exported)
 C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current", "qs_get_observables",
          "qs_vector_length", "qs_active_states", "qs_fft_length", "qs_initial_vector", "qs_residual",
-         "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host")
+         "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
+         "qs_kernel_launches", "qs_profile")
 
 
 def _ptr(a):
@@ -280,6 +290,15 @@ class Solver:
         self._check(self._f("residual")(self._h, V, _ptr(x), _ptr(F), ctypes.byref(ab)), "residual")
         return F, bool(ab.value)
 
+    def profile(self, enable):
+        """Per-family device time (ms) and launch counts since the last call; enable
+        True/False switches event timing on/off, None only reads."""
+        ms = np.zeros(len(KERNEL_FAMILIES))
+        cnt = np.zeros(len(KERNEL_FAMILIES), np.int64)
+        flag = -1 if enable is None else int(bool(enable))
+        self._f("profile")(self._h, flag, _ptr(ms), _ptr(cnt), len(KERNEL_FAMILIES))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_FAMILIES)}
+
     def self_energies(self, x):
         m, nA = self.model, self.nA
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -295,7 +314,7 @@ def invert_batched(A, precision=QS_PREC_FP64, lib=None, prefix="qs_"):
     lib = lib or _lib
     A = np.asarray(A, np.complex128)
     batch, N, _ = A.shape
-    buf = np.ascontiguousarray(A.transpose(0, 2, 1))  # column-major matrices
+    buf = np.array(A.transpose(0, 2, 1), dtype=np.complex128, order="C", copy=True)  # column-major matrices
     info = np.zeros(batch, np.int32)
     rc = getattr(lib, prefix + "invert_batched")(N, batch, _ptr(buf), _ptr(info), precision)
     if rc < 0:
