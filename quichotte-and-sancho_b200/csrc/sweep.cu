@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
         }
         __syncthreads();
         bool singular = false;
+        int first_zero = 0;  // 1 + the first step with a zero pivot (LAPACK's INFO)
         // ---- Gauss-Jordan with row interchanges
         for (int k = 0; k < N; k++) {
             // pivot search
@@ -125,7 +126,10 @@ __global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
                 __syncthreads();
             }
             zc pivot = M[k + (size_t)k * N];
-            if (pivot.x == 0.0 && pivot.y == 0.0) singular = true;
+            if (pivot.x == 0.0 && pivot.y == 0.0) {
+                if (!singular) first_zero = k + 1;
+                singular = true;
+            }
             zc inv = singular ? zc{0.0, 0.0} : crecip(pivot);
             zc f = upd ? M[myrow + (size_t)k * N] : zc{0.0, 0.0};
             __syncthreads();
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
         __syncthreads();
         if (singular && tid == 0) {
             atomicMin(a.info, iw + 1);
-            if (a.info_each) a.info_each[iw - a.iw0] = 1;
+            if (a.info_each) a.info_each[iw - a.iw0] = first_zero;
         }
         // ---- output
         if (a.out_mode == 0) {
