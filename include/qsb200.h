@@ -123,6 +123,23 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
                           int nhist, int maxscf, double tolf, int single_history, int *converged,
                           int *n_iter, double *fmax, qs_scf_step *log, int log_cap);
 
+/* ---- inversion without allocation (no counterpart in the reference) ----
+ * The batched inversion of qs_invert_batched for callers that cannot allocate GPU memory
+ * (their device memory belongs to an enclosing application's pool or arena, or their
+ * loop cannot take the synchronisation of cudaMalloc/cudaFree). A and info are DEVICE
+ * pointers the caller owns: A holds `batch` N x N complex column-major matrices and is
+ * replaced by their inverses; info[b] = 0, or k+1 for a zero pivot at step k. The work
+ * runs asynchronously on `stream` (a cudaStream_t, NULL = legacy default stream); read info
+ * after synchronising. The library allocates nothing: its workspace is a fixed 16 MiB
+ * device array that every GPU loading the library holds until exit. The first call on
+ * each device looks up that array's address (cudaGetSymbolAddress) with the device
+ * current; make this first call before any stream capture. All calls share the array, so
+ * calls that overlap on the GPU (other streams or threads) race: serialise them. Limits:
+ * 1 <= N <= 512 (else QS_ERR_NOALLOC_LIMIT, with a message on stderr). Returns 0 or a
+ * CUDA error (< 0). */
+enum { QS_ERR_NOALLOC_LIMIT = -1001 };
+int qs_invert_batched_noalloc(int N, int batch, double *A, int *info, void *stream);
+
 /* ---- instrumentation (no counterpart in the reference, whose only timer is the
  * wall clock of src/quichotte.f90:50-58) ---- */
 

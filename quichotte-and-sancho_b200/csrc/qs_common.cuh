@@ -198,6 +198,8 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
 int sum_over_energies(qs_handle *h, const zc *d_A, int64_t ld, int ncols, int64_t nrows, zc *d_out);
 int sum_over_energies_real(qs_handle *h, const double *d_A, int64_t ld, int ncols, int64_t nrows, double *d_out);
 int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, zc *d_ws, int ws_slots);
+int invert_batched_ws(cudaStream_t st, int N, int batch, zc *d_A, int *d_min_info, int *d_info_each, zc *d_ws,
+                      int ws_slots);
 int convert_ref_to_dl(cudaStream_t st, int nA, int64_t Nw, const double *ref, double *dl);
 int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, double *ref);
 

@@ -540,6 +540,28 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
     return e == cudaSuccess ? 0 : -(int)e;
 }
 
+// Batched inversion with every matrix in the given global workspace (ws_slots matrices
+// of N x N complex, reused round-robin by the blocks), whatever N is.
+int invert_batched_ws(cudaStream_t st, int N, int batch, zc *d_A, int *d_min_info, int *d_info_each, zc *d_ws,
+                      int ws_slots) {
+    DysonArgs a{};
+    a.N = N;
+    a.iw0 = 0;
+    a.iw1 = batch;
+    a.Ain = d_A;
+    a.out_mode = 1;
+    a.Gout = d_A;
+    a.info = d_min_info;
+    a.info_each = d_info_each;
+    a.ws = d_ws;
+    int nb = std::min(std::min(batch, 148 * 8), ws_slots);
+    if (nb < 1) return -1;
+    count_launch();
+    dyson_gj<<<nb, dyson_threads(N), 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : -(int)e;
+}
+
 // sweep(mode) over all energies (src/scf.f90:280-290).
 //   M_INIT2 / M_SCF2: output into d_out (SCF vector, DL); M_SCF2 subtracts d_x.
 //   M_SCF1 / M_FINAL: per-energy arrays of the handle.

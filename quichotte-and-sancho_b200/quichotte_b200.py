@@ -141,7 +141,10 @@ def kernel_launches():
 C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current", "qs_get_observables",
          "qs_vector_length", "qs_active_states", "qs_fft_length", "qs_initial_vector", "qs_residual",
          "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
-         "qs_kernel_launches", "qs_profile")
+         "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc")
+QS_ERR_NOALLOC_LIMIT = -1001
+_lib.qs_invert_batched_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p]
 
 
 def _ptr(a):
