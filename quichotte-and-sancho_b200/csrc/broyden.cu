@@ -48,15 +48,30 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sh /* [NV][RE
 }
 
 // partials[b] = (max |F|, sum F^2, sum (F-Fold)^2)
-__global__ void vec_norms(const double *__restrict__ F, const double *__restrict__ Fold, int64_t n, double *__restrict__ part) {
+__global__ void __launch_bounds__(256) vec_norms(const double *__restrict__ F, const double *__restrict__ Fold, int64_t n,
+                                                 double *__restrict__ part) {
     __shared__ double sh[3 * 32];
     double mx = 0.0, v[2] = {0.0, 0.0};
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double f = F[i];
+    const int64_t n2 = n / 2;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n2; q += stride) {
+        double2 f = *(const double2 *)(F + 2 * q);
+        mx = fmax(mx, fmax(fabs(f.x), fabs(f.y)));
+        v[0] = fma(f.x, f.x, v[0]);
+        v[0] = fma(f.y, f.y, v[0]);
+        if (Fold) {
+            double2 o = *(const double2 *)(Fold + 2 * q);
+            double d0 = f.x - o.x, d1 = f.y - o.y;
+            v[1] = fma(d0, d0, v[1]);
+            v[1] = fma(d1, d1, v[1]);
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        double f = F[n - 1];
         mx = fmax(mx, fabs(f));
         v[0] = fma(f, f, v[0]);
         if (Fold) {
-            double d = f - Fold[i];
+            double d = f - Fold[n - 1];
             v[1] = fma(d, d, v[1]);
         }
     }
@@ -76,39 +91,117 @@ __global__ void vec_norms(const double *__restrict__ F, const double *__restrict
 // New history pair in slot `slot` plus the Gram column and dF^T F over nh <= NH columns
 // (common/broyden_mixing.f90:103-138,150-156). Single-precision history stores
 // real(dF/||dF||) and real(alpha dF/||dF|| + dx/||dF||); every dot accumulates in FP64.
+// Each thread handles groups of 4 consecutive elements (vector loads); n % 4 elements at
+// the end are handled one by one.
+template <typename HT> struct V4;
+template <> struct V4<float> { using t = float4; };
+template <> struct V4<double> { using t = double4; };
+
+__device__ __forceinline__ double4 ld4(const double *p) {
+    double2 a = *(const double2 *)p, b = *(const double2 *)(p + 2);
+    return double4{a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st4(double *p, double4 v) {
+    *(double2 *)p = double2{v.x, v.y};
+    *(double2 *)(p + 2) = double2{v.z, v.w};
+}
+template <typename HT> __device__ __forceinline__ void hld4(const HT *p, double (&o)[4]);
+template <> __device__ __forceinline__ void hld4<float>(const float *p, double (&o)[4]) {
+    float4 v = *(const float4 *)p;
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <> __device__ __forceinline__ void hld4<double>(const double *p, double (&o)[4]) {
+    double4 v = ld4(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <typename HT> __device__ __forceinline__ void hst4(HT *p, const HT (&v)[4]);
+template <> __device__ __forceinline__ void hst4<float>(float *p, const float (&v)[4]) {
+    *(float4 *)p = float4{v[0], v[1], v[2], v[3]};
+}
+template <> __device__ __forceinline__ void hst4<double>(double *p, const double (&v)[4]) {
+    st4(p, double4{v[0], v[1], v[2], v[3]});
+}
+
+template <typename HT>
+__device__ __forceinline__ void hist_elem(double f, double fo, double xx, double xo, double fnorm, double rf, double alpha,
+                                          HT &dnew, HT &unew) {
+    double d = f - fo, dx = xx - xo;
+    if (sizeof(HT) == 4) {
+        dnew = (HT)(d * rf);
+        unew = (HT)(alpha * d * rf + dx * rf);
+    } else {  // double history: dF = (F - Fold)/fnorm, U = alpha dF + (x - xold)/fnorm
+        double dd = d / fnorm;
+        dnew = (HT)dd;
+        unew = (HT)(alpha * dd + dx / fnorm);
+    }
+}
+
 template <typename HT, int NH>
-__global__ void __launch_bounds__(256) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
-                                                   const double *__restrict__ x, const double *__restrict__ xold,
-                                                   int64_t n, double fnorm, double alpha, HT *__restrict__ dF,
-                                                   HT *__restrict__ U, int slot, int nh, int store,
-                                                   double *__restrict__ part) {
-    __shared__ double sh[2 * NH * 32];
+__global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
+                                                      const double *__restrict__ x, const double *__restrict__ xold,
+                                                      int64_t n, double fnorm, double alpha, HT *__restrict__ dF,
+                                                      HT *__restrict__ U, int slot, int nh, int store,
+                                                      double *__restrict__ part) {
+    __shared__ double sh[2 * NH * 8];
     double g[NH], c[NH];
 #pragma unroll
     for (int k = 0; k < NH; k++) { g[k] = 0.0; c[k] = 0.0; }
     const double rf = 1.0 / fnorm;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double f = F[i];
-        HT dnew = (HT)0;
-        if (store) {
-            double d = f - Fold[i];
-            double dx = x[i] - xold[i];
-            if (sizeof(HT) == 4) {
-                dnew = (HT)(d * rf);
-                U[(int64_t)slot * n + i] = (HT)(alpha * d * rf + dx * rf);
-            } else {  // double history: dF = (F - Fold)/fnorm, U = alpha dF + (x - xold)/fnorm
-                double dd = d / fnorm;
-                dnew = (HT)dd;
-                U[(int64_t)slot * n + i] = (HT)(alpha * dd + dx / fnorm);
-            }
-            dF[(int64_t)slot * n + i] = dnew;
+    const int64_t n4 = n / 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n4 + (n - 4 * n4); q += stride) {
+        const bool vec = q < n4;
+        const int64_t i0 = vec ? 4 * q : 4 * n4 + (q - n4);
+        const int cnt = vec ? 4 : 1;
+        double f[4], dn[4];
+        HT dnew[4] = {0, 0, 0, 0}, unew[4];
+        if (vec) {
+            double4 fv = ld4(F + i0);
+            f[0] = fv.x; f[1] = fv.y; f[2] = fv.z; f[3] = fv.w;
+        } else {
+            f[0] = F[i0];
         }
+        if (store) {
+            double fo[4], xx[4], xo[4];
+            if (vec) {
+                double4 a = ld4(Fold + i0), b = ld4(x + i0), cc = ld4(xold + i0);
+                fo[0] = a.x; fo[1] = a.y; fo[2] = a.z; fo[3] = a.w;
+                xx[0] = b.x; xx[1] = b.y; xx[2] = b.z; xx[3] = b.w;
+                xo[0] = cc.x; xo[1] = cc.y; xo[2] = cc.z; xo[3] = cc.w;
+            } else {
+                fo[0] = Fold[i0]; xx[0] = x[i0]; xo[0] = xold[i0];
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                if (e < cnt) hist_elem<HT>(f[e], fo[e], xx[e], xo[e], fnorm, rf, alpha, dnew[e], unew[e]);
+            if (vec) {
+                hst4<HT>(dF + (int64_t)slot * n + i0, dnew);
+                hst4<HT>(U + (int64_t)slot * n + i0, unew);
+            } else {
+                dF[(int64_t)slot * n + i0] = dnew[0];
+                U[(int64_t)slot * n + i0] = unew[0];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++) dn[e] = (double)dnew[e];
 #pragma unroll
         for (int k = 0; k < NH; k++) {
             if (k < nh) {
-                double dk = (store && k == slot) ? (double)dnew : (double)dF[(int64_t)k * n + i];
-                g[k] = fma(dk, (double)dnew, g[k]);
-                c[k] = fma(dk, f, c[k]);
+                double dk[4];
+                if (store && k == slot) {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) dk[e] = dn[e];
+                } else if (vec) {
+                    hld4<HT>(dF + (int64_t)k * n + i0, dk);
+                } else {
+                    dk[0] = (double)dF[(int64_t)k * n + i0];
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if (e < cnt) {
+                        g[k] = fma(dk[e], dn[e], g[k]);
+                        c[k] = fma(dk[e], f[e], c[k]);
+                    }
             }
         }
     }
@@ -122,15 +215,15 @@ __global__ void __launch_bounds__(256) hist_update(const double *__restrict__ F,
             b += __shfl_down_sync(0xffffffffu, b, o);
         }
         if (lane == 0) {
-            sh[(2 * k) * 32 + wid] = a;
-            sh[(2 * k + 1) * 32 + wid] = b;
+            sh[(2 * k) * 8 + wid] = a;
+            sh[(2 * k + 1) * 8 + wid] = b;
         }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < 2 * nh; t += blockDim.x) {
-        double s = 0.0;
-        for (int w = 0; w < nw; w++) s += sh[t * 32 + w];
-        part[(int64_t)blockIdx.x * 2 * MAXH + t] = s;
+        double s2 = 0.0;
+        for (int w = 0; w < nw; w++) s2 += sh[t * 8 + w];
+        part[(int64_t)blockIdx.x * 2 * MAXH + t] = s2;
     }
 }
 
@@ -147,14 +240,30 @@ static void launch_hist(int nb, cudaStream_t st, const double *F, const double *
         hist_update<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
 }
 
-// x_new = x + alpha F - sum_k gamma_k U_k   (common/broyden_mixing.f90:165-178)
+// x_new = x + alpha F - sum_k gamma_k U_k   (common/broyden_mixing.f90:165-178), the
+// gamma terms subtracted one by one in k order as the reference's loop does
 template <typename HT>
-__global__ void x_update(const double *__restrict__ x, const double *__restrict__ F, const HT *__restrict__ U,
-                         const double *__restrict__ gam, int nh, double alpha, int64_t n, double *__restrict__ xnew) {
+__global__ void __launch_bounds__(256) x_update(const double *__restrict__ x, const double *__restrict__ F,
+                                                const HT *__restrict__ U, const double *__restrict__ gam, int nh,
+                                                double alpha, int64_t n, double *__restrict__ xnew) {
     __shared__ double gs[MAXH];
     if (threadIdx.x < nh) gs[threadIdx.x] = gam[threadIdx.x];
     __syncthreads();
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n4 = n / 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n4; q += stride) {
+        const int64_t i0 = 4 * q;
+        double4 xv = ld4(x + i0), fv = ld4(F + i0);
+        double r[4] = {xv.x + alpha * fv.x, xv.y + alpha * fv.y, xv.z + alpha * fv.z, xv.w + alpha * fv.w};
+        for (int k = 0; k < nh; k++) {
+            double u[4];
+            hld4<HT>(U + (int64_t)k * n + i0, u);
+#pragma unroll
+            for (int e = 0; e < 4; e++) r[e] -= u[e] * gs[k];
+        }
+        st4(xnew + i0, double4{r[0], r[1], r[2], r[3]});
+    }
+    for (int64_t i = 4 * n4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         double xi = x[i] + alpha * F[i];
         for (int k = 0; k < nh; k++) xi -= (double)U[(int64_t)k * n + i] * gs[k];
         xnew[i] = xi;

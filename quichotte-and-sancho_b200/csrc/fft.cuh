@@ -1,5 +1,5 @@
-// fft.cuh -- mixed-radix (2,3,4,5,7,8) Stockham FFT of many short sequences held in
-// shared memory, cooperatively by one thread block.
+// fft.cuh -- mixed-radix (2,3,4,5,7,8) Stockham FFTs of short sequences held in shared
+// memory, one warp per sequence.
 //
 // Conventions are FFTW's, as the reference uses them (src/self_energies.f90:102-103,129,
 // 205,208): sign = -1 is the forward transform sum_j x_j exp(-2 pi i jk/L), sign = +1 the
@@ -11,17 +11,24 @@
 //     v_r = x[j + r L/R] * exp(sign 2 pi i r k / (Ns R)),   r = 0..R-1
 //     v   = DFT_R(v)
 //     y[(j / Ns) Ns R + k + r Ns] = v_r
-// After the last pass the result is in natural order.
+// After the last pass the result is in natural order. A pass is done in place: every lane
+// first loads all inputs of its butterflies into registers, the warp synchronises, then
+// the outputs are written. Only __syncwarp is needed, never a block barrier.
+//
+// Shared-memory index padding: element p of a sequence lives at p + p/8 (one spare complex
+// every 8), which spreads the strided accesses of the early passes over all banks.
 #pragma once
 #include "qs_common.cuh"
 
 namespace qs {
 
+__host__ __device__ __forceinline__ int pidx(int p) { return p + (p >> 3); }
+__host__ __device__ __forceinline__ int padded_len(int L) { return L + (L >> 3) + 1; }
+
 // twiddle W_Nf^m (m in [0, Nf)) for the given sign
 template <typename T>
 __device__ __forceinline__ cplx<T> twid(const cplx<T> *__restrict__ tw, int m, int sign) {
-    cplx<T> w = tw[m];
-    return sign < 0 ? w : conj(w);
+    return sign < 0 ? tw[m] : conj(tw[m]);
 }
 
 // multiply by sign*i
@@ -38,16 +45,16 @@ __device__ __forceinline__ void bfly4(cplx<T> &a0, cplx<T> &a1, cplx<T> &a2, cpl
     a3 = d02 - d13;
 }
 
-template <typename T>
-__device__ __forceinline__ void butterfly(cplx<T> *v, int R, int sign, const cplx<T> *__restrict__ tw, int Nf) {
-    if (R == 2) {
+// DFT of R points in registers
+template <typename T, int R>
+__device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *__restrict__ tw, int Nf) {
+    if constexpr (R == 2) {
         cplx<T> a = v[0], b = v[1];
         v[0] = a + b;
         v[1] = a - b;
-    } else if (R == 4) {
+    } else if constexpr (R == 4) {
         bfly4(v[0], v[1], v[2], v[3], sign);
-    } else if (R == 8) {
-        // even / odd radix-4 halves, then the radix-2 combination with W8^q
+    } else if constexpr (R == 8) {
         cplx<T> e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
         cplx<T> o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
         bfly4(e0, e1, e2, e3, sign);
@@ -65,61 +72,87 @@ __device__ __forceinline__ void butterfly(cplx<T> *v, int R, int sign, const cpl
         v[6] = e2 - t2;
         v[3] = e3 + t3;
         v[7] = e3 - t3;
-    } else {  // 3, 5, 7: direct DFT with table twiddles W_R^m = W_Nf^{m Nf/R}
-        cplx<T> o[7];
-        int st = Nf / R;
+    } else {  // 3, 5, 7: direct DFT with table constants W_R^m = W_Nf^{m Nf/R}
+        cplx<T> o[R];
+        const int st = Nf / R;
+#pragma unroll
         for (int q = 0; q < R; q++) {
             cplx<T> s = v[0];
+#pragma unroll
             for (int r = 1; r < R; r++) {
-                int m = (r * q) % R;
+                const int m = (r * q) % R;
                 if (m == 0) s = s + v[r];
-                else cfma(s, v[r], twid(tw, m * st, sign));
+                else {
+                    cplx<T> w = sign < 0 ? tw[m * st] : conj(tw[m * st]);
+                    cfma(s, v[r], w);
+                }
             }
             o[q] = s;
         }
+#pragma unroll
         for (int q = 0; q < R; q++) v[q] = o[q];
     }
 }
 
-// FFT of nseq sequences of length P.L stored contiguously in buf (sequence s at s*L).
-// tmp has the same size. Returns the buffer that holds the result. Ends with a barrier.
-template <typename T>
-__device__ cplx<T> *smem_fft(cplx<T> *buf, cplx<T> *tmp, int nseq, const FftLen &P, int sign,
-                             const cplx<T> *__restrict__ tw, int Nf) {
-    const int L = P.L;
+// one radix-R pass of a warp, src -> dst (both padded); butterflies are processed one at a
+// time per lane, so only R values are live in registers
+template <typename T, int R>
+__device__ __forceinline__ void warp_pass(const cplx<T> *src, cplx<T> *dst, int L, int Ns, int sign,
+                                          const cplx<T> *__restrict__ tw, int Nf) {
+    const int lane = threadIdx.x & 31;
+    const int nR = L / R;
     const int tws = Nf / L;
-    cplx<T> *a = buf, *b = tmp;
-    int Ns = 1;
-    for (int p = 0; p < P.nrad; p++) {
-        const int R = P.rad[p];
-        const int nR = L / R;
-        const int total = nseq * nR;
-        const int ang = L / (Ns * R);
-        for (int t = threadIdx.x; t < total; t += blockDim.x) {
-            int s = t / nR, j = t - s * nR;
-            const cplx<T> *src = a + (size_t)s * L;
-            cplx<T> *dst = b + (size_t)s * L;
-            int k = j % Ns;
-            cplx<T> v[8];
+    const int ang = L / (Ns * R);
+    for (int j = lane; j < nR; j += 32) {
+        cplx<T> v[R];
 #pragma unroll
-            for (int r = 0; r < 8; r++)
-                if (r < R) {
-                    v[r] = src[j + r * nR];
-                    if (r && k) v[r] = v[r] * twid(tw, (r * k * ang) * tws, sign);
-                }
-            butterfly(v, R, sign, tw, Nf);
-            int idxD = (j / Ns) * Ns * R + k;
+        for (int r = 0; r < R; r++) v[r] = src[pidx(j + r * nR)];
+        const int k = j % Ns;
+        if (k) {
 #pragma unroll
-            for (int r = 0; r < 8; r++)
-                if (r < R) dst[idxD + r * Ns] = v[r];
+            for (int r = 1; r < R; r++) {
+                const int m = (r * k * ang) * tws;
+                v[r] = v[r] * (sign < 0 ? tw[m] : conj(tw[m]));
+            }
         }
-        __syncthreads();
+        dft<T, R>(v, sign, tw, Nf);
+        const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[pidx(idxD + r * Ns)] = v[r];
+    }
+    __syncwarp();
+}
+
+// the whole transform of one padded sequence s by one warp, with the warp's own scratch
+// sequence; the result is left in s
+template <typename T>
+__device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign, const cplx<T> *__restrict__ tw,
+                         int Nf) {
+    cplx<T> *a = s, *b = scratch;
+    const int L = P.L;
+    int Ns = 1;
+    unsigned code = P.code;
+    for (int p = 0; p < P.nrad; p++) {
+        const int R = code & 15u;
+        code >>= 4;
+        switch (R) {
+            case 2: warp_pass<T, 2>(a, b, L, Ns, sign, tw, Nf); break;
+            case 3: warp_pass<T, 3>(a, b, L, Ns, sign, tw, Nf); break;
+            case 4: warp_pass<T, 4>(a, b, L, Ns, sign, tw, Nf); break;
+            case 5: warp_pass<T, 5>(a, b, L, Ns, sign, tw, Nf); break;
+            case 7: warp_pass<T, 7>(a, b, L, Ns, sign, tw, Nf); break;
+            default: warp_pass<T, 8>(a, b, L, Ns, sign, tw, Nf); break;
+        }
         cplx<T> *t = a;
         a = b;
         b = t;
         Ns *= R;
     }
-    return a;
+    if (a != s) {
+        const int lane = threadIdx.x & 31;
+        for (int j = lane; j < L; j += 32) s[pidx(j)] = a[pidx(j)];
+        __syncwarp();
+    }
 }
 
 }  // namespace qs

@@ -68,6 +68,29 @@ template <typename T> __device__ __forceinline__ cplx<T> crecip(cplx<T> a) {
 }
 template <typename D, typename S> __host__ __device__ __forceinline__ cplx<D> cvt(cplx<S> a) { return {(D)a.x, (D)a.y}; }
 
+// FP64 tensor-core MMA, D = A B + D with A 16x16 (row), B 16x8 (col), f64 accumulate.
+// Fragments (g = lane/4, t = lane%4): a_i = A(g + 8(i&1), t + 4(i>>1)), i < 8;
+// b_i = B(t + 4i, g), i < 4; c_i = C(g + 8(i>>1), 2t + (i&1)), i < 4.
+__device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+          "d"(b[2]), "d"(b[3]));
+}
+// complex 16x8 tile update C += A B from split real/imaginary fragments (4 real MMAs)
+__device__ __forceinline__ void zmma16816(double (&cr)[4], double (&ci)[4], const double (&ar)[8], const double (&ai)[8],
+                                          const double (&br)[4], const double (&bi)[4]) {
+    double nai[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) nai[k] = -ai[k];
+    dmma16816(cr, ar, br);
+    dmma16816(cr, nai, bi);
+    dmma16816(ci, ar, bi);
+    dmma16816(ci, ai, br);
+}
+
 constexpr double PI = 3.14159265358979323846;
 constexpr int SMEM_MAX = 232448;  // max dynamic shared memory per block on sm_100 (227 KB)
 
@@ -79,7 +102,8 @@ inline bool dyson_fits_smem(int N) { return (size_t)N * N * 16 + 1536 <= (size_t
 struct FftLen {
     int L;
     int nrad;
-    int rad[24];
+    unsigned code;  // radix of pass p in bits 4p..4p+3
+    int rad[8];     // the same radices (host side)
 };
 
 // Stockham plan for Nf = N1 * N2 and the twiddle table W[k] = exp(-2 pi i k / Nf).

@@ -28,39 +28,46 @@ namespace qs {
 
 // ---------------------------------------------------------------------------------
 // Kernel A: forward length-N1 transforms of the zero-padded element sequences.
+// Block tile: SA adjacent sequences x GA adjacent m2 (SA*16 B contiguous per energy block
+// read, GA*16 B contiguous per Y row written); one warp per sequence.
 // ---------------------------------------------------------------------------------
 template <typename T>
-__global__ void sig2_fwdA(const double *__restrict__ X, int64_t nblk, int n, const int2 *__restrict__ desc, int nY,
-                          FftPlan fp, const cplx<T> *__restrict__ tw, cplx<T> *__restrict__ Y, int SA, int GA) {
+__global__ void __launch_bounds__(256) sig2_fwdA(const double *__restrict__ X, int64_t nblk, int n,
+                                                 const int2 *__restrict__ desc, int nY, FftPlan fp,
+                                                 const cplx<T> *__restrict__ tw, cplx<T> *__restrict__ Y, int SA,
+                                                 int GA) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf;
+    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int s0 = blockIdx.x * SA, m20 = blockIdx.y * GA;
     const int nseq = SA * GA;
     cplx<T> *buf = (cplx<T> *)smem_raw;
-    cplx<T> *tmp = buf + (size_t)nseq * N1;
-    const int total = nseq * N1;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
+    // only m1 < ceil((n - m2)/N2) can be non-zero (zero padding beyond n energies)
+    const int m1max = (n + N2 - 1) / N2;
+    for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int sl = t % SA, r = t / SA;
         int gl = r % GA, m1 = r / GA;
         int s = s0 + sl, m2 = m20 + gl;
         int64_t w = (int64_t)N2 * m1 + m2;
         cplx<T> v{0, 0};
-        if (s < nY && m2 < N2 && w < n) {
+        if (m1 < m1max && s < nY && m2 < N2 && w < n) {
             int2 d = desc[s];
             const double *blk = X + w * nblk;
             v.x = d.x >= 0 ? (T)blk[d.x] : (T)0;
             v.y = (T)blk[d.y];
         }
-        buf[(size_t)(sl * GA + gl) * N1 + m1] = v;
+        buf[(sl * GA + gl) * PL + pidx(m1)] = v;
     }
     __syncthreads();
-    cplx<T> *res = smem_fft(buf, tmp, nseq, fp.p1, -1, tw, Nf);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = warp; q < nseq; q += nw) warp_fft(buf + q * PL, scr, fp.p1, -1, tw, Nf);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GA, r = t / GA;
         int l1 = r % N1, sl = r / N1;
         int s = s0 + sl, m2 = m20 + gl;
         if (s < nY && m2 < N2) {
-            cplx<T> v = res[(size_t)(sl * GA + gl) * N1 + l1] * tw[m2 * l1];
+            cplx<T> v = buf[(sl * GA + gl) * PL + pidx(l1)] * tw[m2 * l1];
             Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = v;
         }
     }
@@ -132,51 +139,55 @@ __device__ __forceinline__ void pair_algebra(const B2<T> &r_ij, const B2<T> &L_i
 
 // ---------------------------------------------------------------------------------
 // Kernel B: spectra, 2x2 algebra, inverse length-N2 transforms, for one site pair
-// (I <= J) and the column pair {c, N1-c}.
+// (I <= J) and the column pair {c, N1-c}. Shared memory: 24 input and 32 output sequences
+// (padded); the transforms are done one sequence per warp.
 // ---------------------------------------------------------------------------------
 template <typename T>
-__global__ void sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V, const int2 *__restrict__ pairs, int nA,
-                         FftPlan fp, const cplx<T> *__restrict__ tw) {
+__global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
+                                                const int2 *__restrict__ pairs, int nA, FftPlan fp,
+                                                const cplx<T> *__restrict__ tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf;
+    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N2);
     const int2 pr = pairs[blockIdx.x];
     const int I = pr.x, J = pr.y, io = 2 * I, jo = 2 * J;
     const int c = blockIdx.y;
     const int cp = (N1 - c) % N1;
     const int ncols = (cp == c) ? 1 : 2;
-    const int cols[2] = {c, cp};
     const bool diag = (I == J);
     const int nfull = nA * nA;
-    auto id_r = [&](int i, int j) { return i + j * nA; };
-    auto id_l = [&](int i, int j) { return nfull + (j * (j + 1)) / 2 + i; };  // i <= j
+    const int nblko = diag ? 1 : 2;
 
-    cplx<T> *Sa = (cplx<T> *)smem_raw;            // 24 N2
-    cplx<T> *Sb = Sa + (size_t)24 * N2;           // 24 N2
-    cplx<T> *O = Sb + (size_t)24 * N2;            // 32 N2: [stage R/L][blk][col][elem][N2]
+    cplx<T> *S = (cplx<T> *)smem_raw;  // 24 sequences: [ci*12 + k]
+    cplx<T> *O = S + 24 * PL;           // 32 sequences: [((stage*2 + b)*2 + ci)*4 + e]
+    cplx<T> *scr = O + 32 * PL + (threadIdx.x >> 5) * PL;  // this warp's scratch
 
-    // 1. load the 12 input sequences of each column
-    const int nin = ncols * 12 * N2;
-    for (int t = threadIdx.x; t < nin; t += blockDim.x) {
+    // 1. the 12 input sequences of each column: R_IJ (k 0-3), R_JI (4-7), L (8-11)
+    for (int t = threadIdx.x; t < ncols * 12 * N2; t += blockDim.x) {
         int m2 = t % N2, r = t / N2;
         int k = r % 12, ci = r / 12;
         int a = k & 1, b = (k >> 1) & 1;
         int sid = -1;
-        if (k < 4) sid = id_r(io + a, jo + b);
-        else if (k < 8) sid = id_r(jo + a, io + b);
-        else if (!diag) sid = id_l(io + a, jo + b);
-        else if (k == 8) sid = id_l(io, io);
-        else if (k == 9) sid = id_l(io, io + 1);
-        else if (k == 10) sid = id_l(io + 1, io + 1);
+        if (k < 4) sid = io + a + (jo + b) * nA;
+        else if (k < 8) sid = jo + a + (io + b) * nA;
+        else if (!diag) sid = nfull + ((jo + b) * (jo + b + 1)) / 2 + io + a;  // upper (io+a, jo+b)
+        else if (k == 8) sid = nfull + (io * (io + 1)) / 2 + io;                   // (io, io)
+        else if (k == 9) sid = nfull + ((io + 1) * (io + 2)) / 2 + io;             // (io, io+1)
+        else if (k == 10) sid = nfull + ((io + 1) * (io + 2)) / 2 + io + 1;        // (io+1, io+1)
         cplx<T> v{0, 0};
-        if (sid >= 0) v = Y[(size_t)sid * Nf + (size_t)cols[ci] * N2 + m2];
-        Sa[(size_t)(ci * 12 + k) * N2 + m2] = v;
+        if (sid >= 0) v = Y[(size_t)sid * Nf + (size_t)(ci ? cp : c) * N2 + m2];
+        S[(ci * 12 + k) * PL + pidx(m2)] = v;
     }
     __syncthreads();
-    cplx<T> *S = smem_fft(Sa, Sb, ncols * 12, fp.p2, -1, tw, Nf);
-    cplx<T> *Fr = (S == Sa) ? Sb : Sa;
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = warp; q < ncols * 12; q += nw) warp_fft(S + q * PL, scr, fp.p2, -1, tw, Nf);
+    __syncthreads();
 
-    auto sv = [&](int ci, int k, int l2) { return S[(size_t)(ci * 12 + k) * N2 + l2]; };
-    // L block of (I,J) at (ci, l2); for I == J the (1,0) element comes from the partner
+    auto sv = [&](int ci, int k, int l2) { return S[(ci * 12 + k) * PL + pidx(l2)]; };
+    auto partner = [&](int ci, int l2, int &pci, int &pl2) {
+        const int col = ci ? cp : c;
+        pci = (ncols == 1) ? 0 : 1 - ci;
+        pl2 = (col == 0) ? (N2 - l2) % N2 : N2 - 1 - l2;
+    };
     auto LIJ = [&](int ci, int l2) {
         B2<T> L;
         if (!diag) {
@@ -185,9 +196,8 @@ __global__ void sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
             L.a[0][1] = sv(ci, 10, l2);
             L.a[1][1] = sv(ci, 11, l2);
         } else {
-            int col = cols[ci];
-            int pci = (ncols == 1) ? 0 : 1 - ci;
-            int pl2 = (col == 0) ? (N2 - l2) % N2 : N2 - 1 - l2;
+            int pci, pl2;
+            partner(ci, l2, pci, pl2);
             L.a[0][0] = sv(ci, 8, l2);
             L.a[0][1] = sv(ci, 9, l2);
             L.a[1][1] = sv(ci, 10, l2);
@@ -203,78 +213,77 @@ __global__ void sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
         R.a[1][1] = sv(ci, base + 3, l2);
         return R;
     };
-    const int nblkout = diag ? 1 : 2;
-    // 2. 2x2 algebra at every position of the loaded columns
-    for (int t = threadIdx.x; t < ncols * N2; t += blockDim.x) {
-        int l2 = t % N2, ci = t / N2;
-        int col = cols[ci];
-        int pci = (ncols == 1) ? 0 : 1 - ci;
-        int pl2 = (col == 0) ? (N2 - l2) % N2 : N2 - 1 - l2;
+    auto put = [&](int b, int ci, int l2, const B2<T> &sR, const B2<T> &sL) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            O[(((0 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sR.a[e & 1][e >> 1];
+            O[(((1 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sL.a[e & 1][e >> 1];
+        }
+    };
+    // 2. 2x2 algebra at every position of the loaded columns (block (I,J), then (J,I))
+    for (int t = threadIdx.x; t < nblko * ncols * N2; t += blockDim.x) {
+        int l2 = t % N2, r = t / N2;
+        int ci = r % ncols, b = r / ncols;
+        int pci, pl2;
+        partner(ci, l2, pci, pl2);
         B2<T> sR, sL;
-        // block (I,J) at l
-        {
-            B2<T> r_ij = RB(ci, 0, l2), L_ij = LIJ(ci, l2), r_ji = RB(pci, 4, pl2);
-            B2<T> L_ji = diag ? LIJ(pci, pl2) : neg2(dag2(L_ij));
-            pair_algebra(r_ij, L_ij, r_ji, L_ji, sR, sL);
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                O[((size_t)((0 * 2 + 0) * 2 + ci) * 4 + e) * N2 + l2] = sR.a[e & 1][e >> 1];
-                O[((size_t)((1 * 2 + 0) * 2 + ci) * 4 + e) * N2 + l2] = sL.a[e & 1][e >> 1];
-            }
-        }
-        if (!diag) {  // block (J,I) at l
+        if (b == 0) {
+            B2<T> L_ij = LIJ(ci, l2);
+            pair_algebra(RB(ci, 0, l2), L_ij, RB(pci, 4, pl2), diag ? LIJ(pci, pl2) : neg2(dag2(L_ij)), sR, sL);
+        } else {
             B2<T> Lp = LIJ(pci, pl2);
-            B2<T> r_ij = RB(ci, 4, l2), L_ij = neg2(dag2(Lp)), r_ji = RB(pci, 0, pl2);
-            pair_algebra(r_ij, L_ij, r_ji, Lp, sR, sL);
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                O[((size_t)((0 * 2 + 1) * 2 + ci) * 4 + e) * N2 + l2] = sR.a[e & 1][e >> 1];
-                O[((size_t)((1 * 2 + 1) * 2 + ci) * 4 + e) * N2 + l2] = sL.a[e & 1][e >> 1];
-            }
+            pair_algebra(RB(ci, 4, l2), neg2(dag2(Lp)), RB(pci, 0, pl2), Lp, sR, sL);
         }
+        put(b, ci, l2, sR, sL);
     }
     __syncthreads();
-    // 3. inverse length-N2 transforms, twiddle, store; stage 0 = Sigma^R, 1 = Sigma^<
-    for (int stage = 0; stage < 2; stage++) {
-        cplx<T> *Os = O + (size_t)stage * 16 * N2;
-        // sequences of this stage: [blk][col][elem] -> only the used (blk, col) ones exist;
-        // transform all 16 (unused ones hold garbage and are not stored)
-        cplx<T> *res = smem_fft(Os, Fr, 16, fp.p2, +1, tw, Nf);
-        const int nout = nblkout * ncols * 4 * N2;
-        for (int t = threadIdx.x; t < nout; t += blockDim.x) {
-            int m2 = t % N2, r = t / N2;
-            int e = r % 4, r2 = r / 4;
-            int ci = r2 % ncols, b = r2 / ncols;
-            int a = e & 1, bb = e >> 1;
-            int row = (b == 0 ? io : jo) + a, colm = (b == 0 ? jo : io) + bb;
-            int col = cols[ci];
-            cplx<T> v = res[((size_t)(b * 2 + ci) * 4 + e) * N2 + m2] * twid(tw, m2 * col, +1);
-            size_t sid = (size_t)stage * nfull + id_r(row, colm);
-            V[sid * Nf + (size_t)col * N2 + m2] = v;
-        }
-        __syncthreads();
+    // 3. inverse length-N2 transforms of the used output sequences, twiddle, store
+    const int nout = 2 * nblko * ncols * 4;  // [stage][b][ci][e] restricted to used b, ci
+    for (int q = warp; q < nout; q += nw) {
+        int e = q % 4, r = q / 4;
+        int ci = r % ncols, r2 = r / ncols;
+        int b = r2 % nblko, stage = r2 / nblko;
+        warp_fft(O + (((stage * 2 + b) * 2 + ci) * 4 + e) * PL, scr, fp.p2, +1, tw, Nf);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nout * N2; t += blockDim.x) {
+        int m2 = t % N2, q = t / N2;
+        int e = q % 4, r = q / 4;
+        int ci = r % ncols, r2 = r / ncols;
+        int b = r2 % nblko, stage = r2 / nblko;
+        int a = e & 1, bb = e >> 1;
+        int row = (b == 0 ? io : jo) + a, colm = (b == 0 ? jo : io) + bb;
+        int col = ci ? cp : c;
+        cplx<T> v = O[(((stage * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(m2)] * twid(tw, m2 * col, +1);
+        size_t sid = (size_t)stage * nfull + row + (size_t)colm * nA;
+        V[sid * Nf + (size_t)col * N2 + m2] = v;
     }
 }
 
 // ---------------------------------------------------------------------------------
 // Kernel C: inverse length-N1 transforms, scaling, first n energies -> Sigma (w-major).
+// Block = one column jo+bb of the output 2x2 block (I,J): the 4 sequences Sigma^R and
+// Sigma^< of rows io, io+1 (two 32 B stores per energy) x GC adjacent m2.
 // ---------------------------------------------------------------------------------
 template <typename T>
-__global__ void sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR, zc *__restrict__ SigL, int nA, int nAs,
-                          int n, const double *__restrict__ Upair, FftPlan fp, const cplx<T> *__restrict__ tw, int GC) {
+__global__ void __launch_bounds__(256) sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
+                                                 zc *__restrict__ SigL, int nA, int nAs, int n,
+                                                 const double *__restrict__ Upair, FftPlan fp,
+                                                 const cplx<T> *__restrict__ tw, int GC) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf;
-    const int I = blockIdx.x % nAs, J = blockIdx.x / nAs;
+    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int bb = blockIdx.x & 1, pairid = blockIdx.x >> 1;
+    const int I = pairid % nAs, J = pairid / nAs;
     const int io = 2 * I, jo = 2 * J;
     const int m20 = blockIdx.y * GC;
     const int nfull = nA * nA;
     const double c = Upair[I + J * nAs];  // U_I U_J hbar^2 (delta/2pi)^2 / Nf, 0 if no interaction
-    const int nseq = 8 * GC;
+    const int nseq = 4 * GC;              // [sl = st*2 + a][gl]
+    const int m1max = (n + N2 - 1) / N2;
     if (c == 0.0) {
         // src/self_energies.f90:167-171: zero blocks
-        const int tot = 8 * GC * N1;
-        for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-            int a = t & 1, bb = (t >> 1) & 1, st = (t >> 2) & 1, r = t >> 3;
+        for (int t = threadIdx.x; t < 4 * GC * m1max; t += blockDim.x) {
+            int a = t & 1, st = (t >> 1) & 1, r = t >> 2;
             int gl = r % GC, m1 = r / GC;
             int m2 = m20 + gl;
             int64_t w = (int64_t)N2 * m1 + m2;
@@ -286,31 +295,30 @@ __global__ void sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR, 
         return;
     }
     cplx<T> *buf = (cplx<T> *)smem_raw;
-    cplx<T> *tmp = buf + (size_t)nseq * N1;
-    const int total = nseq * N1;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
+    for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GC, r = t / GC;
-        int sl = r % 8, l1 = r / 8;
+        int sl = r % 4, l1 = r / 4;
         int m2 = m20 + gl;
-        int e = sl & 3, st = sl >> 2;
-        int a = e & 1, bb = e >> 1;
+        int a = sl & 1, st = sl >> 1;
         cplx<T> v{0, 0};
         if (m2 < N2) {
             size_t sid = (size_t)st * nfull + (io + a) + (size_t)(jo + bb) * nA;
             v = V[sid * Nf + (size_t)l1 * N2 + m2];
         }
-        buf[(size_t)(sl * GC + gl) * N1 + l1] = v;
+        buf[(sl * GC + gl) * PL + pidx(l1)] = v;
     }
     __syncthreads();
-    cplx<T> *res = smem_fft(buf, tmp, nseq, fp.p1, +1, tw, Nf);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int a = t & 1, bb = (t >> 1) & 1, st = (t >> 2) & 1, r = t >> 3;
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = warp; q < nseq; q += nw) warp_fft(buf + q * PL, scr, fp.p1, +1, tw, Nf);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nseq * m1max; t += blockDim.x) {
+        int a = t & 1, st = (t >> 1) & 1, r = t >> 2;
         int gl = r % GC, m1 = r / GC;
         int m2 = m20 + gl;
         int64_t w = (int64_t)N2 * m1 + m2;
         if (m2 < N2 && w < n) {
-            int sl = st * 4 + a + 2 * bb;
-            cplx<T> v = res[(size_t)(sl * GC + gl) * N1 + m1];
+            cplx<T> v = buf[((st * 2 + a) * GC + gl) * PL + pidx(m1)];
             zc *S = st ? SigL : SigR;
             S[w * nfull + (io + a) + (size_t)(jo + bb) * nA] = zc{c * (double)v.x, c * (double)v.y};
         }
@@ -323,9 +331,11 @@ __global__ void sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR, 
 static void factor_len(int L, FftLen &P) {
     P.L = L;
     P.nrad = 0;
+    P.code = 0;
     int m = L;
     for (int r : {8, 4, 2, 3, 5, 7})
         while (m % r == 0) {
+            P.code |= (unsigned)r << (4 * P.nrad);
             P.rad[P.nrad++] = r;
             m /= r;
         }
@@ -407,17 +417,23 @@ int sigma2_setup(qs_handle *h) {
     h->sig2_Upair = dU;
     h->sig2_pairs = dP;
     h->sig2_npairs = (int)pairs.size();
-    // tile sizes
-    int GA = std::min(fp.N2, 8);
-    int SA = std::max(1, std::min(16, 4096 / (fp.N1 * GA)));
-    while (SA * GA * fp.N1 > 4096 && GA > 1) GA /= 2;
+    // tile sizes: one warp per sequence, 64 B contiguous global accesses where possible
+    if (fp.N1 > 512 || fp.N2 > 128) {
+        h->err = "sigma2: FFT length " + std::to_string(fp.Nf) + " needs N1 <= 512 and N2 <= 128";
+        return -1;
+    }
+    const int PL1 = padded_len(fp.N1), PL2 = padded_len(fp.N2);
+    int GA = std::min(fp.N2, 4), SA = 4;
+    while ((size_t)(SA * GA + 8) * PL1 * sizeof(zc) > 112 * 1024 && GA > 1) GA /= 2;
+    while ((size_t)(SA * GA + 8) * PL1 * sizeof(zc) > 112 * 1024 && SA > 1) SA /= 2;
     h->sig2_SA = SA;
     h->sig2_GA = GA;
-    int GC = std::max(1, std::min(fp.N2, 512 / fp.N1));
+    int GC = std::min(fp.N2, 4);
+    while ((size_t)(4 * GC + 8) * PL1 * sizeof(zc) > 112 * 1024 && GC > 1) GC /= 2;
     h->sig2_GC = GC;
-    size_t smA = sizeof(zc) * 2 * (size_t)SA * GA * fp.N1;
-    size_t smB = sizeof(zc) * 80 * (size_t)fp.N2;
-    size_t smC = sizeof(zc) * 2 * (size_t)8 * GC * fp.N1;
+    size_t smA = sizeof(zc) * (size_t)(SA * GA + 8) * PL1;
+    size_t smB = sizeof(zc) * (size_t)(56 + 16) * PL2;
+    size_t smC = sizeof(zc) * (size_t)(4 * GC + 8) * PL1;
     if (smA > SMEM_MAX || smB > SMEM_MAX || smC > SMEM_MAX) {
         h->err = "sigma2: FFT tiles exceed shared memory";
         return -1;
@@ -446,11 +462,11 @@ int sigma2_compute(qs_handle *h, const double *d_x) {
     if (h->sig2_npairs > 0) {
         dim3 gB((unsigned)h->sig2_npairs, (unsigned)(fp.N1 / 2 + 1));
         int pb = prof_begin(h, K_SIG2B);
-        sig2_mid<double><<<gB, 256, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw);
+        sig2_mid<double><<<gB, 512, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw);
         prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
-    dim3 gC((unsigned)(h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
+    dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
     int pc = prof_begin(h, K_SIG2C);
     sig2_invC<double><<<gC, 256, h->sig2_smem[2], h->stream>>>(h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n,
                                                              h->sig2_Upair, fp, h->d_tw, h->sig2_GC);

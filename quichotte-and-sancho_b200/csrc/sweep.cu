@@ -186,6 +186,232 @@ __global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
 }
 
 // ---------------------------------------------------------------------------------
+// Blocked Gauss-Jordan (panel width GJ_B) for matrices held in shared memory. For every
+// panel K = [k0, k0+b): warp 0 factors the N x b panel (pivot search by shuffles, full-row
+// interchanges, scaling and elimination restricted to the panel columns); then the whole
+// block applies the panel's transformation to the other columns as one rank-b update,
+//   A[i, j] += sum_t A[i, K_t] A[K_t, j]            (i, j outside K; register tiles 4 x 4)
+//   A[K, j]  = A[K, K] A[K, j]                       (the pivot rows, one column per thread)
+// which equals the unblocked elimination (row interchanges commute with the deferred update
+// because they act on whole rows). Interchanges are undone on the columns at the end.
+// ---------------------------------------------------------------------------------
+constexpr int GJ_B = 16;  // panel width = the k extent of one FP64 tensor-core MMA
+
+// shared-memory position of element (i, j): column-major with the leading dimension padded
+// to a multiple of 8 units (16 B each) and the unit index XORed with (j mod 8), so that a
+// warp walking along a row (fixed i, consecutive j) hits all banks; columns start on
+// 128-byte boundaries, so the XOR stays inside the column and the map is one-to-one
+__host__ __device__ __forceinline__ int swz_ld(int N) { return ((N + 7) / 8) * 8; }
+__device__ __forceinline__ int swz(int i, int j, int N) { return (i + j * swz_ld(N)) ^ (j & 7); }
+__host__ __device__ __forceinline__ int swz_units(int N) { return N * swz_ld(N); }
+
+// named barrier of the 4 panel warps (ids 1.. are free; 0 is __syncthreads)
+__device__ __forceinline__ void panel_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(512) dyson_bgj(DysonArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N = a.N;
+    zc *M = (zc *)smem_raw;
+    __shared__ unsigned short perm[512];
+    __shared__ double cand_v[4];
+    __shared__ int cand_i[4];
+    __shared__ int first_zero_s;
+    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int mtiles = (N + 15) / 16, ntiles = (N + 7) / 8;
+
+    for (int iw = a.iw0 + blockIdx.x; iw < a.iw1; iw += gridDim.x) {
+        if (a.Ain) {
+            const zc *A = a.Ain + (size_t)(iw - a.iw0) * N * N;
+            for (int idx = tid; idx < N * N; idx += nthr) M[swz(idx % N, idx / N, N)] = A[idx];
+        } else {
+            const double w = a.omega[iw];
+            const zc *SR = a.SigR + (size_t)iw * a.nA * a.nA;
+#pragma unroll 4
+            for (int idx = tid; idx < N * N; idx += nthr) {
+                int i = idx % N, j = idx / N;
+                zc v = a.Hemb[idx];
+                if (a.use_sigma) {
+                    int pi = a.pos[i], pj = a.pos[j];
+                    if (pi >= 0 && pj >= 0) {
+                        zc sg = a.Sig1[idx];
+                        if (a.order2) sg = sg + SR[pi + (size_t)pj * a.nA];
+                        v = v - sg;
+                    }
+                }
+                if (i == j) v.x += w;
+                M[swz(i, j, N)] = v;
+            }
+        }
+        if (tid == 0) first_zero_s = 0;
+        bool singular = false;
+        __syncthreads();
+        for (int k0 = 0; k0 < N; k0 += GJ_B) {
+            const int kb = min(GJ_B, N - k0);
+            // ---- panel factorization by warps 0-3 (one row per thread, named barrier)
+            if (warp < 4) {
+                const int i = tid;  // this thread's row
+                for (int k = k0; k < k0 + kb; k++) {
+                    double v = (i >= k && i < N) ? cabs1(M[swz(i, k, N)]) : -1.0;
+                    int vi = (i >= k && i < N) ? i : N;
+                    warp_argmax(v, vi);
+                    if (lane == 0) {
+                        cand_v[warp] = v;
+                        cand_i[warp] = vi;
+                    }
+                    panel_bar();
+                    double bv = cand_v[0];
+                    int p = cand_i[0];
+#pragma unroll
+                    for (int q = 1; q < 4; q++)
+                        if (cand_v[q] > bv || (cand_v[q] == bv && cand_i[q] < p)) {
+                            bv = cand_v[q];
+                            p = cand_i[q];
+                        }
+                    if (tid == 0) perm[k] = (unsigned short)p;
+                    if (p != k && i < N) {  // thread i swaps column i of rows k and p
+                        zc tt = M[swz(k, i, N)];
+                        M[swz(k, i, N)] = M[swz(p, i, N)];
+                        M[swz(p, i, N)] = tt;
+                    }
+                    panel_bar();
+                    const zc pivot = M[swz(k, k, N)];
+                    if (pivot.x == 0.0 && pivot.y == 0.0 && !singular) {
+                        singular = true;  // every panel thread sees the same pivot
+                        if (tid == 0) first_zero_s = k + 1;
+                    }
+                    const zc inv = singular ? zc{0.0, 0.0} : crecip(pivot);
+                    const zc f = (i < N) ? M[swz(i, k, N)] : zc{0, 0};
+                    panel_bar();
+                    if (i < kb) {
+                        const int c = k0 + i;
+                        zc tt = (c == k) ? zc{1.0, 0.0} : M[swz(k, c, N)];
+                        M[swz(k, c, N)] = tt * inv;
+                    }
+                    panel_bar();
+                    if (i < N && i != k) {
+#pragma unroll
+                        for (int c = 0; c < GJ_B; c++) {
+                            if (c < kb) {
+                                const int cc = k0 + c;
+                                const zc r = M[swz(k, cc, N)];
+                                zc tt = (cc == k) ? zc{0.0, 0.0} : M[swz(i, cc, N)];
+                                tt.x = fma(-f.x, r.x, tt.x);
+                                tt.x = fma(f.y, r.y, tt.x);
+                                tt.y = fma(-f.x, r.y, tt.y);
+                                tt.y = fma(-f.y, r.x, tt.y);
+                                M[swz(i, cc, N)] = tt;
+                            }
+                        }
+                    }
+                    panel_bar();
+                }
+            }
+            __syncthreads();
+            // ---- phase 1: A[i, j] += sum_t A[i, K_t] A[K_t, j], i, j outside K, as complex
+            // 16 x 8 tiles on the FP64 tensor cores (K padded with zeros to 16). N <= 128, so
+            // there are at most 8 row tiles: each warp keeps one row tile's A fragment in
+            // registers and walks a strided set of column tiles.
+            {
+                const int wpr = nwarps / mtiles;  // warps per row tile (>= 2)
+                const int rt = warp / wpr;
+                if (rt < mtiles) {
+                    const int i0 = 16 * rt;
+                    double ar[8], ai[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int r = i0 + g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
+                        zc v = (r < N && c < kb) ? M[swz(r, k0 + c, N)] : zc{0, 0};
+                        ar[q] = v.x;
+                        ai[q] = v.y;
+                    }
+                    for (int ct = warp % wpr; ct < ntiles; ct += wpr) {
+                        const int j0 = 8 * ct;
+                        if (j0 >= k0 && j0 + 8 <= k0 + kb) continue;  // the whole column tile is in K
+                        double br[4], bi[4];
+                        double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const int kr = t4 + 4 * q, c = j0 + g;
+                            zc v = (kr < kb && c < N) ? M[swz(k0 + kr, c, N)] : zc{0, 0};
+                            br[q] = v.x;
+                            bi[q] = v.y;
+                        }
+                        zmma16816(cr, ci, ar, ai, br, bi);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
+                            if (r < N && c < N && (r < k0 || r >= k0 + kb) && (c < k0 || c >= k0 + kb)) {
+                                zc *e = &M[swz(r, c, N)];
+                                *e = zc{e->x + cr[q], e->y + ci[q]};
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- phase 2: the pivot rows, A[K, j] = A[K, K] A[K, j] for j outside K
+            for (int nt = warp; nt < ntiles; nt += nwarps) {
+                const int j0 = 8 * nt;
+                if (j0 >= k0 && j0 + 8 <= k0 + kb) continue;
+                double ar[8], ai[8], br[4], bi[4];
+                double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int r = g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
+                    zc v = (r < kb && c < kb) ? M[swz(k0 + r, k0 + c, N)] : zc{0, 0};
+                    ar[q] = v.x;
+                    ai[q] = v.y;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int kr = t4 + 4 * q, c = j0 + g;
+                    zc v = (kr < kb && c < N) ? M[swz(k0 + kr, c, N)] : zc{0, 0};
+                    br[q] = v.x;
+                    bi[q] = v.y;
+                }
+                zmma16816(cr, ci, ar, ai, br, bi);
+                __syncwarp();  // every lane has read its B fragment before the rows are rewritten
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int r = g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
+                    if (r < kb && c < N && (c < k0 || c >= k0 + kb)) M[swz(k0 + r, c, N)] = zc{cr[q], ci[q]};
+                }
+            }
+            __syncthreads();
+        }
+        // undo the row interchanges by column interchanges in reverse order
+        if (tid < N) {
+            for (int k = N - 1; k >= 0; k--) {
+                int p = perm[k];
+                if (p != k) {
+                    zc tt = M[swz(tid, k, N)];
+                    M[swz(tid, k, N)] = M[swz(tid, p, N)];
+                    M[swz(tid, p, N)] = tt;
+                }
+            }
+        }
+        __syncthreads();
+        if (first_zero_s && tid == 0) {
+            atomicMin(a.info, iw + 1);
+            if (a.info_each) a.info_each[iw - a.iw0] = first_zero_s;
+        }
+        if (a.out_mode == 0) {
+            const int nA = a.nA;
+            zc *G = a.Gout + (size_t)iw * nA * nA;
+            for (int idx = tid; idx < nA * nA; idx += nthr) {
+                int p = idx % nA, q = idx / nA;
+                G[idx] = M[swz(a.act[p], a.act[q], N)];
+            }
+        } else {
+            zc *G = a.Gout + (size_t)(iw - a.iw0) * N * N;
+            for (int idx = tid; idx < N * N; idx += nthr) G[idx] = M[swz(idx % N, idx / N, N)];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Block-level complex GEMM C(MxN) = A(MxK) B(KxN) over 32x32 output tiles, 256 threads,
 // each thread 2x2 outputs. Operands come from loader functors; the store functor gets
 // (i, j, value). With `upper`, tiles strictly below the diagonal are skipped.
@@ -494,8 +720,20 @@ static int dyson_threads(int N) { return N <= 128 ? (N <= 64 ? 256 : 512) : 512;
 static size_t dyson_smem(int N) { return sizeof(zc) * (size_t)N * N; }
 static bool dyson_fits(int N) { return dyson_fits_smem(N); }
 
+static bool use_blocked(int N) { return N >= 16 && N <= 128 && (size_t)swz_units(N) * 16 + 1536 <= (size_t)SMEM_MAX; }
+
 static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
     const int N = a.N;
+    if (use_blocked(N)) {
+        size_t sm = (size_t)swz_units(N) * sizeof(zc);
+        QS_CUDA(h, cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        a.ws = nullptr;
+        int pi = prof_begin(h, K_DYSON);
+        dyson_bgj<<<nblocks, 512, sm, h->stream>>>(a);
+        prof_end(h, pi);
+        QS_CUDA(h, cudaGetLastError());
+        return 0;
+    }
     int thr = dyson_threads(N);
     size_t sm = 0;
     if (dyson_fits(N)) {
@@ -526,6 +764,15 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
     int thr = dyson_threads(N);
     int nb = std::min(batch, 148 * 8);
     size_t sm = 0;
+    if (use_blocked(N)) {
+        sm = (size_t)swz_units(N) * sizeof(zc);
+        cudaError_t e = cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return -(int)e;
+        count_launch();
+        dyson_bgj<<<nb, 512, sm, st>>>(a);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? 0 : -(int)e;
+    }
     if (dyson_fits(N)) {
         sm = dyson_smem(N);
         cudaError_t e = cudaFuncSetAttribute(dyson_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

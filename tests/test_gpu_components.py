@@ -17,7 +17,7 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.mark.parametrize("N", [1, 2, 5, 8, 16, 33, 64, 100, 120, 121, 200])
+@pytest.mark.parametrize("N", [1, 2, 5, 8, 16, 18, 24, 33, 64, 100, 120, 121, 128, 200])
 def test_invert_batched_matches_numpy(N):
     rng = np.random.default_rng(N)
     batch = 37
@@ -108,3 +108,45 @@ def test_device_broyden_matches_oracle_broyden(single):
         # the path to the fixed point, not the fixed point", common/broyden_mixing.f90:21-26)
         tol = (1e-3 * b_[1] + 1e-10) if single else (1e-6 * b_[1] + 1e-12)
         assert abs(a[1] - b_[1]) <= tol
+
+
+def small_helix(delta):
+    return qb.Model.helix(N_ions=3, N_turns=2, hel_length=1.0, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                          lamb=0.05, U_int=0.9, GammaL_up=0.6, GammaL_down=0.4, GammaR=0.5, T=300.0, mu=0.1,
+                          dw=2.0, up=2.0, delta=delta, order=2)
+
+
+def radices(n):
+    out = set()
+    for r in (2, 3, 5, 7):
+        if n % r == 0:
+            out.add(r)
+    return out
+
+
+# energy steps chosen so that the padded FFT lengths cover radices 2, 3, 5 and 7 and both
+# small and large four-step splits
+DELTAS = [0.05, 0.0137, 0.0071, 0.0043, 0.0029]
+
+
+@pytest.mark.parametrize("delta", DELTAS)
+def test_sigma2_and_residual_match_oracle_over_fft_lengths(delta):
+    m = small_helix(delta)
+    gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+    assert gs.Nf == os_.Nf
+    x = os_.initial_vector(0.3)
+    x = x + 1e-3 * np.random.default_rng(1).standard_normal(x.size)
+    SRg, SLg, _ = gs.self_energies(x)
+    SRo, SLo, _ = os_.self_energies(x)
+    assert rel(SRg, SRo) < 1e-12 and rel(SLg, SLo) < 1e-12, (m.n_omega, gs.Nf)
+    Fg, _ = gs.residual(0.3, x)
+    Fo, _ = os_.residual(0.3, x)
+    assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
+
+
+def test_fft_lengths_cover_all_radices():
+    seen = set()
+    for d in DELTAS:
+        m = small_helix(d)
+        seen |= radices(qb.Solver(m).Nf)
+    assert seen == {2, 3, 5, 7}, seen
