@@ -205,16 +205,47 @@ __host__ __device__ __forceinline__ int swz_ld(int N) { return ((N + 7) / 8) * 8
 __device__ __forceinline__ int swz(int i, int j, int N) { return (i + j * swz_ld(N)) ^ (j & 7); }
 __host__ __device__ __forceinline__ int swz_units(int N) { return N * swz_ld(N); }
 
+// 15 warps: one per 8-column tile of a 120-column matrix in the update, and 136 registers a
+// thread for the panel's register-resident rows
+constexpr int BGJ_THREADS = 480;
+
 // named barrier of the 4 panel warps (ids 1.. are free; 0 is __syncthreads)
 __device__ __forceinline__ void panel_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
 
-__global__ void __launch_bounds__(512) dyson_bgj(DysonArgs a) {
+// argmax over a warp with the result in every lane (first maximum wins)
+__device__ __forceinline__ void warp_argmax_all(double &v, int &i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        if (v2 > v || (v2 == v && i2 < i)) {
+            v = v2;
+            i = i2;
+        }
+    }
+}
+
+// Blocked Gauss-Jordan inversion for 16 <= N <= 128 with the matrix in (swizzled) shared
+// memory. Per panel K = [k0, k0 + 16):
+//   panel   warps 0-3, thread i holding row i of the panel columns in registers: per column
+//           k the pivot search, the exchange of rows k and p (the panel part through shared
+//           memory, the rest of the two rows in place), and the elimination restricted to
+//           the panel columns; two 128-thread barriers per column
+//   update  every warp owns 16 x 8 column tiles j outside K: A[i, j] += A[i, K] A[K, j] for
+//           rows i outside K, then A[K, j] = A[K, K] A[K, j], complex products on the FP64
+//           tensor cores; the warp reads its A[K, j] fragment before it rewrites those rows,
+//           so no block barrier separates the two
+// The row interchanges are undone by column interchanges in reverse order at the end.
+__global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N = a.N;
     zc *M = (zc *)smem_raw;
-    __shared__ unsigned short perm[512];
+    // static shared memory stays below 1536 bytes (use_blocked): N = 120 takes the rest
+    __shared__ unsigned char perm[128];
     __shared__ double cand_v[4];
     __shared__ int cand_i[4];
+    __shared__ zc cand_row[4][GJ_B];  // each panel warp's pivot candidate row (panel part)
+    __shared__ zc krow[GJ_B];         // the panel part of row k before the exchange
     __shared__ int first_zero_s;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const int g = lane >> 2, t4 = lane & 3;
@@ -248,121 +279,115 @@ __global__ void __launch_bounds__(512) dyson_bgj(DysonArgs a) {
         __syncthreads();
         for (int k0 = 0; k0 < N; k0 += GJ_B) {
             const int kb = min(GJ_B, N - k0);
-            // ---- panel factorization by warps 0-3 (one row per thread, named barrier)
+            // ---- panel
             if (warp < 4) {
                 const int i = tid;  // this thread's row
-                for (int k = k0; k < k0 + kb; k++) {
-                    double v = (i >= k && i < N) ? cabs1(M[swz(i, k, N)]) : -1.0;
-                    int vi = (i >= k && i < N) ? i : N;
-                    warp_argmax(v, vi);
+                // R[j] holds panel column (c + j) mod 16 at step c: the current column is always
+                // R[0] and the step loop need not be unrolled (padding columns stay zero)
+                zc R[GJ_B];
+#pragma unroll
+                for (int c = 0; c < GJ_B; c++) R[c] = (i < N && c < kb) ? M[swz(i, k0 + c, N)] : zc{0, 0};
+#pragma unroll 1
+                for (int c = 0; c < kb; c++) {
+                    const int k = k0 + c;
+                    const bool valid = (i >= k && i < N);
+                    // every thread prepares 1 / R[0] in case its row becomes the pivot row; the
+                    // division overlaps the pivot search
+                    const bool z = (R[0].x == 0.0 && R[0].y == 0.0);
+                    zc inv_own{0.0, 0.0};
+                    if (!singular && !z) {
+                        const double id = 1.0 / fma(R[0].x, R[0].x, R[0].y * R[0].y);
+                        inv_own = zc{R[0].x * id, -R[0].y * id};
+                    }
+                    // pivot search: the warp maximum of cabs1, then its lowest lane (first maximum)
+                    const double v = valid ? cabs1(R[0]) : -1.0;
+                    double m = v;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                    const unsigned bal = __ballot_sync(0xffffffffu, valid && v == m);
+                    const int wl = bal ? __ffs(bal) - 1 : 32;
                     if (lane == 0) {
-                        cand_v[warp] = v;
-                        cand_i[warp] = vi;
+                        cand_v[warp] = m;
+                        cand_i[warp] = bal ? 32 * warp + wl : N;
+                    }
+                    if (lane == wl) {  // this warp's candidate publishes its scaled row
+#pragma unroll
+                        for (int j = 0; j < GJ_B; j++) cand_row[warp][j] = (j == 0) ? inv_own : R[j] * inv_own;
+                    }
+                    if (i == k) {
+#pragma unroll
+                        for (int j = 0; j < GJ_B; j++) krow[j] = R[j];
                     }
                     panel_bar();
                     double bv = cand_v[0];
-                    int p = cand_i[0];
+                    int p = cand_i[0], wb = 0;
 #pragma unroll
-                    for (int q = 1; q < 4; q++)
-                        if (cand_v[q] > bv || (cand_v[q] == bv && cand_i[q] < p)) {
-                            bv = cand_v[q];
-                            p = cand_i[q];
+                    for (int q = 1; q < 4; q++) {
+                        const double cv = cand_v[q];
+                        const int ci = cand_i[q];
+                        if (cv > bv || (cv == bv && ci < p)) {
+                            bv = cv;
+                            p = ci;
+                            wb = q;
                         }
-                    if (tid == 0) perm[k] = (unsigned short)p;
-                    if (p != k && i < N) {  // thread i swaps column i of rows k and p
+                    }
+                    if (bv == 0.0 && !singular) {  // cabs1 of the pivot is zero
+                        singular = true;           // every panel thread sees the same pivot
+                        if (tid == 0) first_zero_s = k + 1;
+                    }
+                    if (tid == 0) perm[k] = (unsigned char)p;
+                    // rows k and p exchange their panel parts: row p takes the old row k
+                    if (p != k && i == p) {
+#pragma unroll
+                        for (int j = 0; j < GJ_B; j++) R[j] = krow[j];
+                    }
+                    // eliminate with the scaled pivot row S (S_0 = 1 / pivot), then rotate the
+                    // window by one column
+                    const zc *S = cand_row[wb];
+                    const zc f = R[0];
+                    const bool pr = (i == k);
+                    zc first;
+#pragma unroll
+                    for (int j = 0; j < GJ_B; j++) {
+                        const zc r = S[j];
+                        zc tt;
+                        if (pr) {
+                            tt = r;
+                        } else {
+                            tt = (j == 0) ? zc{0.0, 0.0} : R[j];
+                            tt.x = fma(-f.x, r.x, tt.x);
+                            tt.x = fma(f.y, r.y, tt.x);
+                            tt.y = fma(-f.x, r.y, tt.y);
+                            tt.y = fma(-f.y, r.x, tt.y);
+                        }
+                        if (j == 0) first = tt;
+                        else R[j - 1] = tt;
+                    }
+                    R[GJ_B - 1] = first;
+                    // the rest of rows k and p (thread i moves column i, its own earlier
+                    // exchanges first)
+                    if (p != k && i < N && (i < k0 || i >= k0 + kb)) {
                         zc tt = M[swz(k, i, N)];
                         M[swz(k, i, N)] = M[swz(p, i, N)];
                         M[swz(p, i, N)] = tt;
                     }
-                    panel_bar();
-                    const zc pivot = M[swz(k, k, N)];
-                    if (pivot.x == 0.0 && pivot.y == 0.0 && !singular) {
-                        singular = true;  // every panel thread sees the same pivot
-                        if (tid == 0) first_zero_s = k + 1;
-                    }
-                    const zc inv = singular ? zc{0.0, 0.0} : crecip(pivot);
-                    const zc f = (i < N) ? M[swz(i, k, N)] : zc{0, 0};
-                    panel_bar();
-                    if (i < kb) {
-                        const int c = k0 + i;
-                        zc tt = (c == k) ? zc{1.0, 0.0} : M[swz(k, c, N)];
-                        M[swz(k, c, N)] = tt * inv;
-                    }
-                    panel_bar();
-                    if (i < N && i != k) {
-#pragma unroll
-                        for (int c = 0; c < GJ_B; c++) {
-                            if (c < kb) {
-                                const int cc = k0 + c;
-                                const zc r = M[swz(k, cc, N)];
-                                zc tt = (cc == k) ? zc{0.0, 0.0} : M[swz(i, cc, N)];
-                                tt.x = fma(-f.x, r.x, tt.x);
-                                tt.x = fma(f.y, r.y, tt.x);
-                                tt.y = fma(-f.x, r.y, tt.y);
-                                tt.y = fma(-f.y, r.x, tt.y);
-                                M[swz(i, cc, N)] = tt;
-                            }
-                        }
-                    }
-                    panel_bar();
+                    panel_bar();  // cand_row and krow are rewritten by the next column
                 }
-            }
-            __syncthreads();
-            // ---- phase 1: A[i, j] += sum_t A[i, K_t] A[K_t, j], i, j outside K, as complex
-            // 16 x 8 tiles on the FP64 tensor cores (K padded with zeros to 16). N <= 128, so
-            // there are at most 8 row tiles: each warp keeps one row tile's A fragment in
-            // registers and walks a strided set of column tiles.
-            {
-                const int wpr = nwarps / mtiles;  // warps per row tile (>= 2)
-                const int rt = warp / wpr;
-                if (rt < mtiles) {
-                    const int i0 = 16 * rt;
-                    double ar[8], ai[8];
+                // after kb steps R[j] holds column (kb + j) mod 16
+                if (i < N) {
 #pragma unroll
-                    for (int q = 0; q < 8; q++) {
-                        const int r = i0 + g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
-                        zc v = (r < N && c < kb) ? M[swz(r, k0 + c, N)] : zc{0, 0};
-                        ar[q] = v.x;
-                        ai[q] = v.y;
-                    }
-                    for (int ct = warp % wpr; ct < ntiles; ct += wpr) {
-                        const int j0 = 8 * ct;
-                        if (j0 >= k0 && j0 + 8 <= k0 + kb) continue;  // the whole column tile is in K
-                        double br[4], bi[4];
-                        double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            const int kr = t4 + 4 * q, c = j0 + g;
-                            zc v = (kr < kb && c < N) ? M[swz(k0 + kr, c, N)] : zc{0, 0};
-                            br[q] = v.x;
-                            bi[q] = v.y;
-                        }
-                        zmma16816(cr, ci, ar, ai, br, bi);
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
-                            if (r < N && c < N && (r < k0 || r >= k0 + kb) && (c < k0 || c >= k0 + kb)) {
-                                zc *e = &M[swz(r, c, N)];
-                                *e = zc{e->x + cr[q], e->y + ci[q]};
-                            }
-                        }
+                    for (int j = 0; j < GJ_B; j++) {
+                        const int c = (kb + j) & (GJ_B - 1);
+                        if (c < kb) M[swz(i, k0 + c, N)] = R[j];
                     }
                 }
             }
             __syncthreads();
-            // ---- phase 2: the pivot rows, A[K, j] = A[K, K] A[K, j] for j outside K
-            for (int nt = warp; nt < ntiles; nt += nwarps) {
-                const int j0 = 8 * nt;
-                if (j0 >= k0 && j0 + 8 <= k0 + kb) continue;
-                double ar[8], ai[8], br[4], bi[4];
-                double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const int r = g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
-                    zc v = (r < kb && c < kb) ? M[swz(k0 + r, k0 + c, N)] : zc{0, 0};
-                    ar[q] = v.x;
-                    ai[q] = v.y;
-                }
+            // ---- update, one 16 x 8 column tile at a time per warp
+            for (int ct = warp; ct < ntiles; ct += nwarps) {
+                const int j0 = 8 * ct;
+                if (j0 >= k0 && j0 + 8 <= k0 + kb) continue;  // the whole column tile is in K
+                double br[4], bi[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int kr = t4 + 4 * q, c = j0 + g;
@@ -370,8 +395,44 @@ __global__ void __launch_bounds__(512) dyson_bgj(DysonArgs a) {
                     br[q] = v.x;
                     bi[q] = v.y;
                 }
+#pragma unroll 1
+                for (int rt = 0; rt < mtiles; rt++) {
+                    const int i0 = 16 * rt;
+                    if (i0 >= k0 && i0 + 16 <= k0 + kb) continue;  // the whole row tile is in K
+                    double ar[8], ai[8], cr[4], ci[4];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int r = i0 + g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
+                        zc v = (r < N && c < kb) ? M[swz(r, k0 + c, N)] : zc{0, 0};
+                        ar[q] = v.x;
+                        ai[q] = v.y;
+                    }
+                    bool own[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
+                        own[q] = r < N && c < N && (r < k0 || r >= k0 + kb) && (c < k0 || c >= k0 + kb);
+                        zc v = own[q] ? M[swz(r, c, N)] : zc{0, 0};
+                        cr[q] = v.x;
+                        ci[q] = v.y;
+                    }
+                    zmma16816(cr, ci, ar, ai, br, bi);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
+                        if (own[q]) M[swz(r, c, N)] = zc{cr[q], ci[q]};
+                    }
+                }
+                // the pivot rows
+                double ar[8], ai[8], cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int r = g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
+                    zc v = (r < kb && c < kb) ? M[swz(k0 + r, k0 + c, N)] : zc{0, 0};
+                    ar[q] = v.x;
+                    ai[q] = v.y;
+                }
                 zmma16816(cr, ci, ar, ai, br, bi);
-                __syncwarp();  // every lane has read its B fragment before the rows are rewritten
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int r = g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
@@ -729,7 +790,7 @@ static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
         QS_CUDA(h, cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         a.ws = nullptr;
         int pi = prof_begin(h, K_DYSON);
-        dyson_bgj<<<nblocks, 512, sm, h->stream>>>(a);
+        dyson_bgj<<<nblocks, BGJ_THREADS, sm, h->stream>>>(a);
         prof_end(h, pi);
         QS_CUDA(h, cudaGetLastError());
         return 0;
@@ -769,7 +830,7 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
         cudaError_t e = cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return -(int)e;
         count_launch();
-        dyson_bgj<<<nb, 512, sm, st>>>(a);
+        dyson_bgj<<<nb, BGJ_THREADS, sm, st>>>(a);
         e = cudaGetLastError();
         return e == cudaSuccess ? 0 : -(int)e;
     }
