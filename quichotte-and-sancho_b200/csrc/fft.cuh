@@ -11,12 +11,16 @@
 //     v_r = x[j + r L/R] * exp(sign 2 pi i r k / (Ns R)),   r = 0..R-1
 //     v   = DFT_R(v)
 //     y[(j / Ns) Ns R + k + r Ns] = v_r
-// After the last pass the result is in natural order. A pass is done in place: every lane
-// first loads all inputs of its butterflies into registers, the warp synchronises, then
-// the outputs are written. Only __syncwarp is needed, never a block barrier.
+// After the last pass the result is in natural order. The passes alternate between the
+// sequence and a scratch sequence of the warp (out of place), so only __syncwarp is needed
+// between them, never a block barrier.
 //
 // Shared-memory index padding: element p of a sequence lives at p + p/8 (one spare complex
 // every 8), which spreads the strided accesses of the early passes over all banks.
+//
+// Twiddles come from a table twL[m] = exp(-2 pi i m / L), m < L, that the calling kernel
+// keeps in shared memory (L1 holds little next to the sequence buffers, and a global table
+// read at stride Nf/L would miss it on every access).
 #pragma once
 #include "qs_common.cuh"
 
@@ -25,9 +29,8 @@ namespace qs {
 __host__ __device__ __forceinline__ int pidx(int p) { return p + (p >> 3); }
 __host__ __device__ __forceinline__ int padded_len(int L) { return L + (L >> 3) + 1; }
 
-// twiddle W_Nf^m (m in [0, Nf)) for the given sign
-template <typename T>
-__device__ __forceinline__ cplx<T> twid(const cplx<T> *__restrict__ tw, int m, int sign) {
+// twiddle W^m from a table for the given sign
+template <typename T> __device__ __forceinline__ cplx<T> twid(const cplx<T> *tw, int m, int sign) {
     return sign < 0 ? tw[m] : conj(tw[m]);
 }
 
@@ -47,7 +50,7 @@ __device__ __forceinline__ void bfly4(cplx<T> &a0, cplx<T> &a1, cplx<T> &a2, cpl
 
 // DFT of R points in registers
 template <typename T, int R>
-__device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *__restrict__ tw, int Nf) {
+__device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *twL, int L) {
     if constexpr (R == 2) {
         cplx<T> a = v[0], b = v[1];
         v[0] = a + b;
@@ -72,9 +75,9 @@ __device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *__
         v[6] = e2 - t2;
         v[3] = e3 + t3;
         v[7] = e3 - t3;
-    } else {  // 3, 5, 7: direct DFT with table constants W_R^m = W_Nf^{m Nf/R}
+    } else {  // 3, 5, 7: direct DFT with table constants W_R^m = W_L^{m L/R}
         cplx<T> o[R];
-        const int st = Nf / R;
+        const int st = L / R;
 #pragma unroll
         for (int q = 0; q < R; q++) {
             cplx<T> s = v[0];
@@ -83,7 +86,7 @@ __device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *__
                 const int m = (r * q) % R;
                 if (m == 0) s = s + v[r];
                 else {
-                    cplx<T> w = sign < 0 ? tw[m * st] : conj(tw[m * st]);
+                    cplx<T> w = sign < 0 ? twL[m * st] : conj(twL[m * st]);
                     cfma(s, v[r], w);
                 }
             }
@@ -98,10 +101,9 @@ __device__ __forceinline__ void dft(cplx<T> (&v)[R], int sign, const cplx<T> *__
 // time per lane, so only R values are live in registers
 template <typename T, int R>
 __device__ __forceinline__ void warp_pass(const cplx<T> *src, cplx<T> *dst, int L, int Ns, int sign,
-                                          const cplx<T> *__restrict__ tw, int Nf) {
+                                          const cplx<T> *twL) {
     const int lane = threadIdx.x & 31;
     const int nR = L / R;
-    const int tws = Nf / L;
     const int ang = L / (Ns * R);
     for (int j = lane; j < nR; j += 32) {
         cplx<T> v[R];
@@ -111,11 +113,11 @@ __device__ __forceinline__ void warp_pass(const cplx<T> *src, cplx<T> *dst, int 
         if (k) {
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                const int m = (r * k * ang) * tws;
-                v[r] = v[r] * (sign < 0 ? tw[m] : conj(tw[m]));
+                const int m = r * k * ang;  // < R Ns ang = L
+                v[r] = v[r] * (sign < 0 ? twL[m] : conj(twL[m]));
             }
         }
-        dft<T, R>(v, sign, tw, Nf);
+        dft<T, R>(v, sign, twL, L);
         const int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
         for (int r = 0; r < R; r++) dst[pidx(idxD + r * Ns)] = v[r];
@@ -124,10 +126,9 @@ __device__ __forceinline__ void warp_pass(const cplx<T> *src, cplx<T> *dst, int 
 }
 
 // the whole transform of one padded sequence s by one warp, with the warp's own scratch
-// sequence; the result is left in s
+// sequence and the length-L twiddle table twL; the result is left in s
 template <typename T>
-__device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign, const cplx<T> *__restrict__ tw,
-                         int Nf) {
+__device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign, const cplx<T> *twL) {
     cplx<T> *a = s, *b = scratch;
     const int L = P.L;
     int Ns = 1;
@@ -136,12 +137,12 @@ __device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign
         const int R = code & 15u;
         code >>= 4;
         switch (R) {
-            case 2: warp_pass<T, 2>(a, b, L, Ns, sign, tw, Nf); break;
-            case 3: warp_pass<T, 3>(a, b, L, Ns, sign, tw, Nf); break;
-            case 4: warp_pass<T, 4>(a, b, L, Ns, sign, tw, Nf); break;
-            case 5: warp_pass<T, 5>(a, b, L, Ns, sign, tw, Nf); break;
-            case 7: warp_pass<T, 7>(a, b, L, Ns, sign, tw, Nf); break;
-            default: warp_pass<T, 8>(a, b, L, Ns, sign, tw, Nf); break;
+            case 2: warp_pass<T, 2>(a, b, L, Ns, sign, twL); break;
+            case 3: warp_pass<T, 3>(a, b, L, Ns, sign, twL); break;
+            case 4: warp_pass<T, 4>(a, b, L, Ns, sign, twL); break;
+            case 5: warp_pass<T, 5>(a, b, L, Ns, sign, twL); break;
+            case 7: warp_pass<T, 7>(a, b, L, Ns, sign, twL); break;
+            default: warp_pass<T, 8>(a, b, L, Ns, sign, twL); break;
         }
         cplx<T> *t = a;
         a = b;
@@ -152,6 +153,70 @@ __device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign
         const int lane = threadIdx.x & 31;
         for (int j = lane; j < L; j += 32) s[pidx(j)] = a[pidx(j)];
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Power-of-two lengths L = 64, 128, 256 with compile-time passes: the warp transforms
+// P = 256 / L sequences at once (sequence q at s + q ps, q < nvalid), every lane holding 8
+// complex values per pass, in place (all loads of a pass precede its stores; no scratch).
+// Passes: radix 8 (Ns = 1), radix 8 (Ns = 8), then radix L / 64 (Ns = 64) when L > 64.
+// ---------------------------------------------------------------------------------
+template <typename T, int L, int R, int Ns>
+__device__ __forceinline__ void pow2_pass(cplx<T> *s, int ps, int nvalid, int sign, const cplx<T> *twL) {
+    constexpr int nR = L / R;  // butterflies per sequence
+    constexpr int U = 8 / R;   // butterflies per lane
+    constexpr int ang = L / (Ns * R);
+    const int lane = threadIdx.x & 31;
+    cplx<T> v[U][R];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int b = lane + 32 * u, sq = b / nR, j = b % nR;
+        const cplx<T> *x = s + sq * ps;
+#pragma unroll
+        for (int r = 0; r < R; r++) v[u][r] = (sq < nvalid) ? x[pidx(j + r * nR)] : cplx<T>{0, 0};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int b = lane + 32 * u, sq = b / nR, j = b % nR;
+        const int k = j % Ns;
+        if (Ns > 1 && k) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[u][r] = v[u][r] * twid(twL, r * k * ang, sign);
+        }
+        dft<T, R>(v[u], sign, twL, L);
+        cplx<T> *x = s + sq * ps;
+        const int idxD = (j / Ns) * Ns * R + k;
+        if (sq < nvalid) {
+#pragma unroll
+            for (int r = 0; r < R; r++) x[pidx(idxD + r * Ns)] = v[u][r];
+        }
+    }
+    __syncwarp();
+}
+
+template <typename T, int L>
+__device__ __forceinline__ void warp_fft_pow2(cplx<T> *s, int ps, int nvalid, int sign, const cplx<T> *twL) {
+    static_assert(L == 64 || L == 128 || L == 256, "power-of-two lengths 64..256");
+    pow2_pass<T, L, 8, 1>(s, ps, nvalid, sign, twL);
+    pow2_pass<T, L, 8, 8>(s, ps, nvalid, sign, twL);
+    if constexpr (L > 64) pow2_pass<T, L, L / 64, 64>(s, ps, nvalid, sign, twL);
+}
+
+// number of sequences one warp transforms per call for length L (1 on the generic path)
+__host__ __device__ __forceinline__ int fft_group(int L) { return (L == 64 || L == 128 || L == 256) ? 256 / L : 1; }
+
+// Transform the group of up to fft_group(L) sequences at s + q ps (q < nvalid) by the
+// calling warp; scratch is used by the generic path (one sequence per call).
+template <typename T>
+__device__ __forceinline__ void warp_fft_group(cplx<T> *s, int ps, int nvalid, cplx<T> *scratch, const FftLen &P,
+                                               int sign, const cplx<T> *twL) {
+    switch (P.L) {
+        case 64: warp_fft_pow2<T, 64>(s, ps, nvalid, sign, twL); break;
+        case 128: warp_fft_pow2<T, 128>(s, ps, nvalid, sign, twL); break;
+        case 256: warp_fft_pow2<T, 256>(s, ps, nvalid, sign, twL); break;
+        default: warp_fft(s, scratch, P, sign, twL); break;
     }
 }
 

@@ -31,17 +31,22 @@ namespace qs {
 // Block tile: SA adjacent sequences x GA adjacent m2 (SA*16 B contiguous per energy block
 // read, GA*16 B contiguous per Y row written); one warp per sequence.
 // ---------------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) sig2_fwdA(const double *__restrict__ X, int64_t nblk, int n,
+// N1C > 0: compile-time N1 (power of two) with 4 x 4 tiles, so the index arithmetic of the
+// load and store loops reduces to shifts and masks; N1C = 0: any N1 and tile.
+template <typename T, int N1C>
+__global__ void __launch_bounds__(256, 2) sig2_fwdA(const double *__restrict__ X, int64_t nblk, int n,
                                                  const int2 *__restrict__ desc, int nY, FftPlan fp,
-                                                 const cplx<T> *__restrict__ tw, cplx<T> *__restrict__ Y, int SA,
-                                                 int GA) {
+                                                 const cplx<T> *__restrict__ tw, cplx<T> *__restrict__ Y, int SA_rt,
+                                                 int GA_rt) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int N1 = N1C ? N1C : fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int SA = N1C ? 4 : SA_rt, GA = N1C ? 4 : GA_rt;
     const int s0 = blockIdx.x * SA, m20 = blockIdx.y * GA;
     const int nseq = SA * GA;
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
+    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
     // only m1 < ceil((n - m2)/N2) can be non-zero (zero padding beyond n energies)
     const int m1max = (n + N2 - 1) / N2;
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
@@ -60,7 +65,10 @@ __global__ void __launch_bounds__(256) sig2_fwdA(const double *__restrict__ X, i
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = warp; q < nseq; q += nw) warp_fft(buf + q * PL, scr, fp.p1, -1, tw, Nf);
+    {
+        const int G = fft_group(N1);
+        for (int q = warp * G; q < nseq; q += nw * G) warp_fft_group(buf + q * PL, PL, min(G, nseq - q), scr, fp.p1, -1, twL);
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GA, r = t / GA;
@@ -137,31 +145,37 @@ __device__ __forceinline__ void pair_algebra(const B2<T> &r_ij, const B2<T> &L_i
     sL = mm2(L_ij, adj2(chiL));
 }
 
+// asynchronous 16-byte (8-byte for float) copy global -> shared; zero-fill when !valid
+template <typename T> __device__ __forceinline__ void cp_async_elem(cplx<T> *dst, const cplx<T> *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(cplx<T>) == 16) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------------------------
 // Kernel B: spectra, 2x2 algebra, inverse length-N2 transforms, for one site pair
-// (I <= J) and the column pair {c, N1-c}. Shared memory: 24 input and 32 output sequences
-// (padded); the transforms are done one sequence per warp.
+// (I <= J) and the column pair {c, N1-c} per work item. Persistent blocks walk the items;
+// the 24 input sequences of the next item are copied asynchronously into the second input
+// buffer while the current item is transformed. Shared memory: 2 x 24 input and 32 output
+// sequences (padded), one scratch sequence per warp and the twiddle tables; one warp per
+// transform (or per group of transforms, for the power-of-two lengths).
 // ---------------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
-                                                const int2 *__restrict__ pairs, int nA, FftPlan fp,
-                                                const cplx<T> *__restrict__ tw) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N2);
-    const int2 pr = pairs[blockIdx.x];
-    const int I = pr.x, J = pr.y, io = 2 * I, jo = 2 * J;
-    const int c = blockIdx.y;
-    const int cp = (N1 - c) % N1;
+template <typename T, int N2C>
+__device__ __forceinline__ void mid_load(const cplx<T> *__restrict__ Y, cplx<T> *S, int item, int ncp,
+                                         const int2 *__restrict__ pairs, int nA, const FftPlan &fp, int PL) {
+    const int N1 = fp.N1, N2 = N2C ? N2C : fp.N2, Nf = fp.Nf;
+    const int2 pr = pairs[item / ncp];
+    const int io = 2 * pr.x, jo = 2 * pr.y;
+    const bool diag = (pr.x == pr.y);
+    const int c = item % ncp, cp = (N1 - c) % N1;
     const int ncols = (cp == c) ? 1 : 2;
-    const bool diag = (I == J);
     const int nfull = nA * nA;
-    const int nblko = diag ? 1 : 2;
-
-    cplx<T> *S = (cplx<T> *)smem_raw;  // 24 sequences: [ci*12 + k]
-    cplx<T> *O = S + 24 * PL;           // 32 sequences: [((stage*2 + b)*2 + ci)*4 + e]
-    cplx<T> *scr = O + 32 * PL + (threadIdx.x >> 5) * PL;  // this warp's scratch
-
-    // 1. the 12 input sequences of each column: R_IJ (k 0-3), R_JI (4-7), L (8-11)
+    // the 12 input sequences of each column: R_IJ (k 0-3), R_JI (4-7), L (8-11)
     for (int t = threadIdx.x; t < ncols * 12 * N2; t += blockDim.x) {
         int m2 = t % N2, r = t / N2;
         int k = r % 12, ci = r / 12;
@@ -173,90 +187,134 @@ __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, c
         else if (k == 8) sid = nfull + (io * (io + 1)) / 2 + io;                   // (io, io)
         else if (k == 9) sid = nfull + ((io + 1) * (io + 2)) / 2 + io;             // (io, io+1)
         else if (k == 10) sid = nfull + ((io + 1) * (io + 2)) / 2 + io + 1;        // (io+1, io+1)
-        cplx<T> v{0, 0};
-        if (sid >= 0) v = Y[(size_t)sid * Nf + (size_t)(ci ? cp : c) * N2 + m2];
-        S[(ci * 12 + k) * PL + pidx(m2)] = v;
+        const cplx<T> *src = sid >= 0 ? Y + (size_t)sid * Nf + (size_t)(ci ? cp : c) * N2 + m2 : Y;
+        cp_async_elem(S + (ci * 12 + k) * PL + pidx(m2), src, sid >= 0);
     }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = warp; q < ncols * 12; q += nw) warp_fft(S + q * PL, scr, fp.p2, -1, tw, Nf);
-    __syncthreads();
+}
 
-    auto sv = [&](int ci, int k, int l2) { return S[(ci * 12 + k) * PL + pidx(l2)]; };
-    auto partner = [&](int ci, int l2, int &pci, int &pl2) {
-        const int col = ci ? cp : c;
-        pci = (ncols == 1) ? 0 : 1 - ci;
-        pl2 = (col == 0) ? (N2 - l2) % N2 : N2 - 1 - l2;
-    };
-    auto LIJ = [&](int ci, int l2) {
-        B2<T> L;
-        if (!diag) {
-            L.a[0][0] = sv(ci, 8, l2);
-            L.a[1][0] = sv(ci, 9, l2);
-            L.a[0][1] = sv(ci, 10, l2);
-            L.a[1][1] = sv(ci, 11, l2);
-        } else {
+// N2C > 0: compile-time N2 (power of two); N2C = 0: any N2
+template <typename T, int N2C>
+__global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
+                                                const int2 *__restrict__ pairs, int nA, FftPlan fp,
+                                                const cplx<T> *__restrict__ tw, int nitems) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N1 = fp.N1, N2 = N2C ? N2C : fp.N2, Nf = fp.Nf, PL = padded_len(N2);
+    const int ncp = N1 / 2 + 1;
+    const int nfull = nA * nA;
+    cplx<T> *S0 = (cplx<T> *)smem_raw;  // 2 x 24 sequences: [ci*12 + k]
+    cplx<T> *O = S0 + 48 * PL;          // 32 sequences: [((stage*2 + b)*2 + ci)*4 + e]
+    cplx<T> *scr = O + 32 * PL + (threadIdx.x >> 5) * PL;  // this warp's scratch
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    cplx<T> *twL = O + (32 + nw) * PL;  // W_N2^m, m < N2
+    cplx<T> *twc = twL + N2;            // W_Nf^{m2 col} of the item's two columns
+    for (int m = threadIdx.x; m < N2; m += blockDim.x) twL[m] = tw[(size_t)m * N1];
+    const int G = fft_group(N2);
+
+    if (blockIdx.x < nitems) mid_load<T, N2C>(Y, S0, blockIdx.x, ncp, pairs, nA, fp, PL);
+    cp_async_commit();
+    int cur = 0;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int nxt = item + gridDim.x;
+        if (nxt < nitems) mid_load<T, N2C>(Y, S0 + (cur ^ 1) * 24 * PL, nxt, ncp, pairs, nA, fp, PL);
+        cp_async_commit();
+        cp_async_wait1();  // this thread's copies of the current item have landed
+        __syncthreads();
+        cplx<T> *S = S0 + cur * 24 * PL;
+        const int2 pr = pairs[item / ncp];
+        const int I = pr.x, J = pr.y, io = 2 * I, jo = 2 * J;
+        const int c = item % ncp;
+        const int cp = (N1 - c) % N1;
+        const int ncols = (cp == c) ? 1 : 2;
+        const bool diag = (I == J);
+        const int nblko = diag ? 1 : 2;
+        for (int t = threadIdx.x; t < 2 * N2; t += blockDim.x)  // used after two barriers
+            twc[t] = tw[(size_t)(t % N2) * ((t < N2) ? c : cp)];
+
+        for (int q = warp * G; q < ncols * 12; q += nw * G)
+            warp_fft_group(S + q * PL, PL, min(G, ncols * 12 - q), scr, fp.p2, -1, twL);
+        __syncthreads();
+
+        auto sv = [&](int ci, int k, int l2) { return S[(ci * 12 + k) * PL + pidx(l2)]; };
+        auto partner = [&](int ci, int l2, int &pci, int &pl2) {
+            const int col = ci ? cp : c;
+            pci = (ncols == 1) ? 0 : 1 - ci;
+            pl2 = (col == 0) ? (N2 - l2) % N2 : N2 - 1 - l2;
+        };
+        auto LIJ = [&](int ci, int l2) {
+            B2<T> L;
+            if (!diag) {
+                L.a[0][0] = sv(ci, 8, l2);
+                L.a[1][0] = sv(ci, 9, l2);
+                L.a[0][1] = sv(ci, 10, l2);
+                L.a[1][1] = sv(ci, 11, l2);
+            } else {
+                int pci, pl2;
+                partner(ci, l2, pci, pl2);
+                L.a[0][0] = sv(ci, 8, l2);
+                L.a[0][1] = sv(ci, 9, l2);
+                L.a[1][1] = sv(ci, 10, l2);
+                L.a[1][0] = -conj(sv(pci, 9, pl2));
+            }
+            return L;
+        };
+        auto RB = [&](int ci, int base, int l2) {
+            B2<T> R;
+            R.a[0][0] = sv(ci, base + 0, l2);
+            R.a[1][0] = sv(ci, base + 1, l2);
+            R.a[0][1] = sv(ci, base + 2, l2);
+            R.a[1][1] = sv(ci, base + 3, l2);
+            return R;
+        };
+        auto put = [&](int b, int ci, int l2, const B2<T> &sR, const B2<T> &sL) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                O[(((0 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sR.a[e & 1][e >> 1];
+                O[(((1 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sL.a[e & 1][e >> 1];
+            }
+        };
+        // 2x2 algebra at every position of the loaded columns (block (I,J), then (J,I));
+        // ncols and nblko are 1 or 2
+        for (int t = threadIdx.x; t < nblko * ncols * N2; t += blockDim.x) {
+            int l2 = t % N2, r = t / N2;
+            int ci = (ncols == 2) ? (r & 1) : 0, b = (ncols == 2) ? (r >> 1) : r;
             int pci, pl2;
             partner(ci, l2, pci, pl2);
-            L.a[0][0] = sv(ci, 8, l2);
-            L.a[0][1] = sv(ci, 9, l2);
-            L.a[1][1] = sv(ci, 10, l2);
-            L.a[1][0] = -conj(sv(pci, 9, pl2));
+            B2<T> sR, sL;
+            if (b == 0) {
+                B2<T> L_ij = LIJ(ci, l2);
+                pair_algebra(RB(ci, 0, l2), L_ij, RB(pci, 4, pl2), diag ? LIJ(pci, pl2) : neg2(dag2(L_ij)), sR, sL);
+            } else {
+                B2<T> Lp = LIJ(pci, pl2);
+                pair_algebra(RB(ci, 4, l2), neg2(dag2(Lp)), RB(pci, 0, pl2), Lp, sR, sL);
+            }
+            put(b, ci, l2, sR, sL);
         }
-        return L;
-    };
-    auto RB = [&](int ci, int base, int l2) {
-        B2<T> R;
-        R.a[0][0] = sv(ci, base + 0, l2);
-        R.a[1][0] = sv(ci, base + 1, l2);
-        R.a[0][1] = sv(ci, base + 2, l2);
-        R.a[1][1] = sv(ci, base + 3, l2);
-        return R;
-    };
-    auto put = [&](int b, int ci, int l2, const B2<T> &sR, const B2<T> &sL) {
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            O[(((0 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sR.a[e & 1][e >> 1];
-            O[(((1 * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(l2)] = sL.a[e & 1][e >> 1];
+        __syncthreads();
+        // inverse length-N2 transforms of the used output sequences; groups of G <= 4
+        // sequences share (stage, b, ci) and are adjacent in O (e, e+1, ..)
+        const int nout = 2 * nblko * ncols * 4;  // [stage][b][ci][e] restricted to used b, ci
+        for (int q = warp * G; q < nout; q += nw * G) {
+            int e = q % 4, r = q / 4;
+            int ci = (ncols == 2) ? (r & 1) : 0, r2 = (ncols == 2) ? (r >> 1) : r;
+            int b = (nblko == 2) ? (r2 & 1) : 0, stage = (nblko == 2) ? (r2 >> 1) : r2;
+            warp_fft_group(O + (((stage * 2 + b) * 2 + ci) * 4 + e) * PL, PL, G, scr, fp.p2, +1, twL);
         }
-    };
-    // 2. 2x2 algebra at every position of the loaded columns (block (I,J), then (J,I))
-    for (int t = threadIdx.x; t < nblko * ncols * N2; t += blockDim.x) {
-        int l2 = t % N2, r = t / N2;
-        int ci = r % ncols, b = r / ncols;
-        int pci, pl2;
-        partner(ci, l2, pci, pl2);
-        B2<T> sR, sL;
-        if (b == 0) {
-            B2<T> L_ij = LIJ(ci, l2);
-            pair_algebra(RB(ci, 0, l2), L_ij, RB(pci, 4, pl2), diag ? LIJ(pci, pl2) : neg2(dag2(L_ij)), sR, sL);
-        } else {
-            B2<T> Lp = LIJ(pci, pl2);
-            pair_algebra(RB(ci, 4, l2), neg2(dag2(Lp)), RB(pci, 0, pl2), Lp, sR, sL);
+        __syncthreads();
+        // twiddle W_Nf^{-m2 col}, store
+        for (int t = threadIdx.x; t < nout * N2; t += blockDim.x) {
+            int m2 = t % N2, q = t / N2;
+            int e = q % 4, r = q / 4;
+            int ci = (ncols == 2) ? (r & 1) : 0, r2 = (ncols == 2) ? (r >> 1) : r;
+            int b = (nblko == 2) ? (r2 & 1) : 0, stage = (nblko == 2) ? (r2 >> 1) : r2;
+            int a = e & 1, bb = e >> 1;
+            int row = (b == 0 ? io : jo) + a, colm = (b == 0 ? jo : io) + bb;
+            int col = ci ? cp : c;
+            cplx<T> v = O[(((stage * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(m2)] * conj(twc[ci * N2 + m2]);
+            size_t sid = (size_t)stage * nfull + row + (size_t)colm * nA;
+            V[sid * Nf + (size_t)col * N2 + m2] = v;
         }
-        put(b, ci, l2, sR, sL);
-    }
-    __syncthreads();
-    // 3. inverse length-N2 transforms of the used output sequences, twiddle, store
-    const int nout = 2 * nblko * ncols * 4;  // [stage][b][ci][e] restricted to used b, ci
-    for (int q = warp; q < nout; q += nw) {
-        int e = q % 4, r = q / 4;
-        int ci = r % ncols, r2 = r / ncols;
-        int b = r2 % nblko, stage = r2 / nblko;
-        warp_fft(O + (((stage * 2 + b) * 2 + ci) * 4 + e) * PL, scr, fp.p2, +1, tw, Nf);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < nout * N2; t += blockDim.x) {
-        int m2 = t % N2, q = t / N2;
-        int e = q % 4, r = q / 4;
-        int ci = r % ncols, r2 = r / ncols;
-        int b = r2 % nblko, stage = r2 / nblko;
-        int a = e & 1, bb = e >> 1;
-        int row = (b == 0 ? io : jo) + a, colm = (b == 0 ? jo : io) + bb;
-        int col = ci ? cp : c;
-        cplx<T> v = O[(((stage * 2 + b) * 2 + ci) * 4 + e) * PL + pidx(m2)] * twid(tw, m2 * col, +1);
-        size_t sid = (size_t)stage * nfull + row + (size_t)colm * nA;
-        V[sid * Nf + (size_t)col * N2 + m2] = v;
+        __syncthreads();  // S[cur], O and twc are rewritten by the next items
+        cur ^= 1;
     }
 }
 
@@ -265,13 +323,15 @@ __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, c
 // Block = one column jo+bb of the output 2x2 block (I,J): the 4 sequences Sigma^R and
 // Sigma^< of rows io, io+1 (two 32 B stores per energy) x GC adjacent m2.
 // ---------------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256) sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
+// N1C > 0: compile-time N1 (power of two) with GC = 4; N1C = 0: any N1 and GC
+template <typename T, int N1C>
+__global__ void __launch_bounds__(256, 2) sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
                                                  zc *__restrict__ SigL, int nA, int nAs, int n,
                                                  const double *__restrict__ Upair, FftPlan fp,
-                                                 const cplx<T> *__restrict__ tw, int GC) {
+                                                 const cplx<T> *__restrict__ tw, int GC_rt) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N1 = fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int N1 = N1C ? N1C : fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int GC = N1C ? 4 : GC_rt;
     const int bb = blockIdx.x & 1, pairid = blockIdx.x >> 1;
     const int I = pairid % nAs, J = pairid / nAs;
     const int io = 2 * I, jo = 2 * J;
@@ -296,6 +356,8 @@ __global__ void __launch_bounds__(256) sig2_invC(const cplx<T> *__restrict__ V, 
     }
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
+    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GC, r = t / GC;
         int sl = r % 4, l1 = r / 4;
@@ -310,7 +372,10 @@ __global__ void __launch_bounds__(256) sig2_invC(const cplx<T> *__restrict__ V, 
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = warp; q < nseq; q += nw) warp_fft(buf + q * PL, scr, fp.p1, +1, tw, Nf);
+    {
+        const int G = fft_group(N1);
+        for (int q = warp * G; q < nseq; q += nw * G) warp_fft_group(buf + q * PL, PL, min(G, nseq - q), scr, fp.p1, +1, twL);
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < nseq * m1max; t += blockDim.x) {
         int a = t & 1, st = (t >> 1) & 1, r = t >> 2;
@@ -349,6 +414,34 @@ static int good_fft_size(int nmin) {
             while (m % r == 0) m /= r;
         if (m == 1) return n;
     }
+}
+
+// the kernel instantiations for a plan: compile-time lengths for the power-of-two splits
+using FwdAFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, zc *, int, int);
+using MidFn = void (*)(const zc *, zc *, const int2 *, int, FftPlan, const zc *, int);
+using InvCFn = void (*)(const zc *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
+static FwdAFn pick_fwdA(int N1, int SA, int GA) {
+    if (SA == 4 && GA == 4) switch (N1) {
+            case 64: return sig2_fwdA<double, 64>;
+            case 128: return sig2_fwdA<double, 128>;
+            case 256: return sig2_fwdA<double, 256>;
+        }
+    return sig2_fwdA<double, 0>;
+}
+static MidFn pick_mid(int N2) {
+    switch (N2) {
+        case 64: return sig2_mid<double, 64>;
+        case 128: return sig2_mid<double, 128>;
+    }
+    return sig2_mid<double, 0>;
+}
+static InvCFn pick_invC(int N1, int GC) {
+    if (GC == 4) switch (N1) {
+            case 64: return sig2_invC<double, 64>;
+            case 128: return sig2_invC<double, 128>;
+            case 256: return sig2_invC<double, 256>;
+        }
+    return sig2_invC<double, 0>;
 }
 
 int sigma2_setup(qs_handle *h) {
@@ -431,16 +524,18 @@ int sigma2_setup(qs_handle *h) {
     int GC = std::min(fp.N2, 4);
     while ((size_t)(4 * GC + 8) * PL1 * sizeof(zc) > 112 * 1024 && GC > 1) GC /= 2;
     h->sig2_GC = GC;
-    size_t smA = sizeof(zc) * (size_t)(SA * GA + 8) * PL1;
-    size_t smB = sizeof(zc) * (size_t)(56 + 16) * PL2;
-    size_t smC = sizeof(zc) * (size_t)(4 * GC + 8) * PL1;
+    size_t smA = sizeof(zc) * ((size_t)(SA * GA + 8) * PL1 + fp.N1);
+    size_t smB = sizeof(zc) * ((size_t)(2 * 24 + 32 + 16) * PL2 + 3 * fp.N2);
+    size_t smC = sizeof(zc) * ((size_t)(4 * GC + 8) * PL1 + fp.N1);
     if (smA > SMEM_MAX || smB > SMEM_MAX || smC > SMEM_MAX) {
         h->err = "sigma2: FFT tiles exceed shared memory";
         return -1;
     }
-    QS_CUDA(h, cudaFuncSetAttribute(sig2_fwdA<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-    QS_CUDA(h, cudaFuncSetAttribute(sig2_mid<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-    QS_CUDA(h, cudaFuncSetAttribute(sig2_invC<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA(fp.N1, SA, GA), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smA));
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_mid(fp.N2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC(fp.N1, GC), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smC));
     h->sig2_smem[0] = smA;
     h->sig2_smem[1] = smB;
     h->sig2_smem[2] = smC;
@@ -455,20 +550,22 @@ int sigma2_compute(qs_handle *h, const double *d_x) {
     const int nA = h->nA;
     dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
     int pa = prof_begin(h, K_SIG2A);
-    sig2_fwdA<double><<<gA, 256, h->sig2_smem[0], h->stream>>>(d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw,
+    pick_fwdA(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, h->sig2_smem[0], h->stream>>>(d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw,
                                                              h->d_Y, h->sig2_SA, h->sig2_GA);
     prof_end(h, pa);
     QS_CUDA(h, cudaGetLastError());
     if (h->sig2_npairs > 0) {
-        dim3 gB((unsigned)h->sig2_npairs, (unsigned)(fp.N1 / 2 + 1));
+        const int nitems = h->sig2_npairs * (fp.N1 / 2 + 1);
+        const int gB = std::min(nitems, 148);  // persistent: one block per SM
         int pb = prof_begin(h, K_SIG2B);
-        sig2_mid<double><<<gB, 512, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw);
+        pick_mid(fp.N2)<<<gB, 512, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw,
+                                                                 nitems);
         prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
     dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
     int pc = prof_begin(h, K_SIG2C);
-    sig2_invC<double><<<gC, 256, h->sig2_smem[2], h->stream>>>(h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n,
+    pick_invC(fp.N1, h->sig2_GC)<<<gC, 256, h->sig2_smem[2], h->stream>>>(h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n,
                                                              h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
     prof_end(h, pc);
     QS_CUDA(h, cudaGetLastError());

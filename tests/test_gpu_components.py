@@ -144,6 +144,24 @@ def test_sigma2_and_residual_match_oracle_over_fft_lengths(delta):
     assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
 
 
+# energy steps whose padded FFT lengths are powers of two: Nf = 4096 (64 x 64), 8192
+# (128 x 64), 16384 (128 x 128), 32768 (256 x 128), the specialised length-64/128/256
+# transforms of both four-step stages
+POW2_DELTAS = [0.0037309, 0.0018609, 0.0009293, 0.0004655]
+
+
+@pytest.mark.parametrize("delta", POW2_DELTAS)
+def test_sigma2_power_of_two_fft_lengths_match_oracle(delta):
+    m = small_helix(delta)
+    gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+    assert gs.Nf == os_.Nf and gs.Nf & (gs.Nf - 1) == 0
+    x = os_.initial_vector(0.3)
+    x = x + 1e-3 * np.random.default_rng(2).standard_normal(x.size)
+    SRg, SLg, _ = gs.self_energies(x)
+    SRo, SLo, _ = os_.self_energies(x)
+    assert rel(SRg, SRo) < 1e-12 and rel(SLg, SLo) < 1e-12, (m.n_omega, gs.Nf)
+
+
 def test_fft_lengths_cover_all_radices():
     seen = set()
     for d in DELTAS:
