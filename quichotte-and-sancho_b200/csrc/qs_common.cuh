@@ -71,8 +71,9 @@ template <typename D, typename S> __host__ __device__ __forceinline__ cplx<D> cv
 // FP64 tensor-core MMA, D = A B + D with A 16x16 (row), B 16x8 (col), f64 accumulate.
 // Fragments (g = lane/4, t = lane%4): a_i = A(g + 8(i&1), t + 4(i>>1)), i < 8;
 // b_i = B(t + 4i, g), i < 4; c_i = C(g + 8(i>>1), 2t + (i&1)), i < 4.
+// (not volatile: the compiler may schedule independent MMAs between dependent ones)
 __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
         "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
         : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])

@@ -587,6 +587,219 @@ __global__ void __launch_bounds__(256) keldysh_scf2(KeldyshArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------------
+// The same step on the FP64 tensor cores for 48 <= nA <= 128: T = G^r SL and the upper
+// triangle of G^< = T G^r^dagger as complex m16n8k16 MMAs (4 real MMAs per complex tile),
+// operands padded to 128 and staged through shared memory in 16-wide k panels by cp.async,
+// double-buffered. 8 warps, one block per SM walking the energies; a warp owns a 32-row
+// block of 8-column tiles. SL and T go through two scratch matrices of the block (L2).
+// ---------------------------------------------------------------------------------
+constexpr int KD_MP = 128, KD_LDA = 130, KD_LDN = 20;  // padded order; [k][m] / [n][k] panel strides
+constexpr int KD_ASZ = 16 * KD_LDA, KD_BSZ = KD_MP * KD_LDN, KD_STAGE = KD_ASZ + KD_BSZ;
+constexpr size_t KD_SMEM = 2 * KD_STAGE * sizeof(zc);
+
+__device__ __forceinline__ void cpa16(void *dst, const void *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+// C(m0 + 0..31, n0 + 0..8NT-1) = A B over k < nA. A: nA x nA column-major. BT = false: B(k, n)
+// = Bm[k + n nA] staged [n][k]; BT = true: B(k, n) = conj(Bm[n + k nA]) staged [k][n]. Only
+// columns nlo..nhi-1 of B are staged. Every thread of the block calls it (the panel copies);
+// warps with !active skip the MMAs.
+template <int NT, bool BT>
+__device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__restrict__ Bm, int nA, int nlo, int nhi,
+                                        int m0, int n0, bool active, zc *sm, double (&cr)[2][NT][4],
+                                        double (&ci)[2][NT][4]) {
+    const int tid = threadIdx.x, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int nk = (nA + 15) / 16, nw = nhi - nlo;
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NT; ni++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) cr[mi][ni][q] = ci[mi][ni][q] = 0.0;
+    auto load = [&](int kc, int st) {
+        zc *As = sm + st * KD_STAGE, *Bs = As + KD_ASZ;
+        const int k0 = kc * 16;
+        for (int idx = tid; idx < 16 * KD_MP; idx += blockDim.x) {
+            const int m = idx & (KD_MP - 1), kk = idx >> 7;
+            const bool v = m < nA && k0 + kk < nA;
+            cpa16(&As[kk * KD_LDA + m], v ? A + m + (size_t)(k0 + kk) * nA : A, v);
+        }
+        for (int idx = tid; idx < 16 * nw; idx += blockDim.x) {
+            if (!BT) {
+                const int kk = idx & 15, nn = nlo + (idx >> 4);
+                const bool v = nn < nA && k0 + kk < nA;
+                cpa16(&Bs[nn * KD_LDN + kk], v ? Bm + (k0 + kk) + (size_t)nn * nA : Bm, v);
+            } else {
+                const int nn = nlo + idx % nw, kk = idx / nw;
+                const bool v = nn < nA && k0 + kk < nA;
+                cpa16(&Bs[kk * KD_LDA + nn], v ? Bm + nn + (size_t)(k0 + kk) * nA : Bm, v);
+            }
+        }
+    };
+    load(0, 0);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    for (int kc = 0; kc < nk; kc++) {
+        if (kc + 1 < nk) load(kc + 1, (kc + 1) & 1);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        if (active) {
+            const zc *As = sm + (kc & 1) * KD_STAGE, *Bs = As + KD_ASZ;
+            double ar[2][8], ai[2][8];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const zc v = As[(t4 + 4 * (q >> 1)) * KD_LDA + m0 + 16 * mi + g + 8 * (q & 1)];
+                    ar[mi][q] = v.x;
+                    ai[mi][q] = v.y;
+                }
+#pragma unroll
+            for (int ni = 0; ni < NT; ni++) {
+                const int c0 = n0 + 8 * ni;
+                double br[4], bi[4], nbi[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const zc v = BT ? Bs[(t4 + 4 * q) * KD_LDA + c0 + g] : Bs[(c0 + g) * KD_LDN + t4 + 4 * q];
+                    br[q] = v.x;
+                    bi[q] = BT ? -v.y : v.y;
+                    nbi[q] = -bi[q];
+                }
+                // the two row tiles interleaved: dependent MMAs are three apart
+                dmma16816(cr[0][ni], ar[0], br);
+                dmma16816(cr[1][ni], ar[1], br);
+                dmma16816(ci[0][ni], ar[0], bi);
+                dmma16816(ci[1][ni], ar[1], bi);
+                dmma16816(cr[0][ni], ai[0], nbi);
+                dmma16816(cr[1][ni], ai[1], nbi);
+                dmma16816(ci[0][ni], ai[0], br);
+                dmma16816(ci[1][ni], ai[1], br);
+            }
+        }
+        __syncthreads();  // the stage is refilled two chunks later
+    }
+}
+
+__global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    zc *sm = (zc *)smem_raw;
+    const int nA = a.nA, nfull = nA * nA;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    zc *T = a.Tws + (size_t)(2 * blockIdx.x) * nfull;
+    zc *S = T + nfull;
+    const int64_t offL = 2 * (int64_t)nfull, offD = offL + (int64_t)nA * (nA - 1);
+    for (int iw = blockIdx.x; iw < a.n; iw += gridDim.x) {
+        const zc *G = a.G + (size_t)iw * nfull;
+        const double w = a.omega[iw];
+        const double fL = fermi_d(w, a.V, a.mu, a.beta), fR = fermi_d(w, 0.0, a.mu, a.beta);
+        const zc *SL2 = a.SigL ? a.SigL + (size_t)iw * nfull : nullptr;
+        // SL = i (fL GamL_s + fR GamR_s) / hbar  (+ Sigma2^<)   (src/scf.f90:333-336); the
+        // loads of 8 elements a thread are issued before their stores
+        for (int base = threadIdx.x; base < nfull; base += 8 * blockDim.x) {
+            zc gl[8], gr[8], s2[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int idx = base + u * blockDim.x;
+                const bool v = idx < nfull;
+                gl[u] = v ? a.GamLs[idx] : zc{0, 0};
+                gr[u] = v ? a.GamRs[idx] : zc{0, 0};
+                s2[u] = (v && SL2) ? SL2[idx] : zc{0, 0};
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int idx = base + u * blockDim.x;
+                if (idx < nfull) S[idx] = zc{-(fL * gl[u].y + fR * gr[u].y) + s2[u].x, fL * gl[u].x + fR * gr[u].x + s2[u].y};
+            }
+        }
+        __threadfence_block();
+        __syncthreads();
+        // T = G SL, in two column halves of 64
+        for (int hh = 0; hh < 2; hh++) {
+            if (64 * hh >= nA) break;
+            double cr[2][4][4], ci[2][4][4];
+            const int m0 = 32 * (warp & 3), n0 = 64 * hh + 32 * (warp >> 2);
+            kd_gemm<4, false>(G, S, nA, 64 * hh, 64 * hh + 64, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int r = m0 + 16 * mi + g + 8 * (q >> 1), c = n0 + 8 * ni + 2 * t4 + (q & 1);
+                        if (r < nA && c < nA) T[r + (size_t)c * nA] = zc{cr[mi][ni][q], ci[mi][ni][q]};
+                    }
+        }
+        __threadfence_block();
+        __syncthreads();
+        double *blk = a.out + (size_t)iw * a.nblk;
+        const double *xb = a.xsub ? a.xsub + (size_t)iw * a.nblk : nullptr;
+        auto put = [&](int r, int c, double vr, double vi) {
+            if (r >= nA || c >= nA || r > c) return;
+            if (r < c) {
+                const int64_t o = offL + 2 * ((int64_t)c * (c - 1) / 2 + r);
+                blk[o] = xb ? vr - xb[o] : vr;
+                blk[o + 1] = xb ? vi - xb[o + 1] : vi;
+            } else {
+                blk[offD + r] = xb ? vi - xb[offD + r] : vi;
+                if (a.gLd) a.gLd[(size_t)iw * nA + r] = zc{vr, vi};
+            }
+        };
+        // upper triangle of G^< = T G^dagger: warp w takes the 32 x 32 block (bi, bj) =
+        // (0,0) (0,1) (1,1) (0,2) (1,2) (2,2) (0,3) (1,3) ...
+        {
+            const int bi = (0x10210100 >> (4 * warp)) & 15, bj = (0x33222110 >> (4 * warp)) & 15;
+            double cr[2][4][4], ci[2][4][4];
+            const int m0 = 32 * bi, n0 = 32 * bj;
+            kd_gemm<4, true>(T, G, nA, 0, min(nA, KD_MP), m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        put(m0 + 16 * mi + g + 8 * (q >> 1), n0 + 8 * ni + 2 * t4 + (q & 1), cr[mi][ni][q], ci[mi][ni][q]);
+        }
+        // ... and (2,3), (3,3) as 32 x 8 strips, four warps each
+        if (nA > 96) {
+            double cr[2][1][4], ci[2][1][4];
+            const int m0 = 32 * (2 + (warp >> 2)), n0 = 96 + 8 * (warp & 3);
+            kd_gemm<1, true>(T, G, nA, 96, KD_MP, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    put(m0 + 16 * mi + g + 8 * (q >> 1), n0 + 2 * t4 + (q & 1), cr[mi][0][q], ci[mi][0][q]);
+        }
+        // G^r part of the block (8 elements a thread in flight)
+        for (int base = threadIdx.x; base < nfull; base += 8 * blockDim.x) {
+            zc gv[8];
+            double xr[8], xi[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int idx = base + u * blockDim.x;
+                const bool v = idx < nfull;
+                gv[u] = v ? G[idx] : zc{0, 0};
+                xr[u] = (v && xb) ? xb[2 * idx] : 0.0;
+                xi[u] = (v && xb) ? xb[2 * idx + 1] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int idx = base + u * blockDim.x;
+                if (idx < nfull) {
+                    blk[2 * idx] = gv[u].x - xr[u];
+                    blk[2 * idx + 1] = gv[u].y - xi[u];
+                }
+            }
+        }
+        if (a.gRd)
+            for (int i = threadIdx.x; i < nA; i += blockDim.x) a.gRd[(size_t)iw * nA + i] = G[i + (size_t)i * nA];
+        __syncthreads();  // S and T are rewritten for the next energy
+    }
+}
+
 struct FinalArgs {
     int N, nS, nA, nCL, N_sites, N_atoms, iw0, iw1, mode;
     const zc *G;  // full G per energy of the chunk
@@ -912,8 +1125,16 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
         int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
-        int pi = prof_begin(h, K_KELDYSH);
-        keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
+        int pi;
+        const int nbt = std::min(n, 148);
+        if (nA >= 48 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt)) {
+            QS_CUDA(h, cudaFuncSetAttribute(keldysh_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KD_SMEM));
+            pi = prof_begin(h, K_KELDYSH);
+            keldysh_tc<<<nbt, 256, KD_SMEM, h->stream>>>(k);
+        } else {
+            pi = prof_begin(h, K_KELDYSH);
+            keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
+        }
         prof_end(h, pi);
         QS_CUDA(h, cudaGetLastError());
         return 0;

@@ -89,6 +89,27 @@ def test_residual_matches_oracle(case):
     assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
 
 
+# helices whose active blocks (nA = 56, 100, 120) take the tensor-core Keldysh kernel,
+# including orders that are not multiples of 16 or 32
+LARGE_HELICES = [(7, 4), (10, 5), (10, 6)]
+
+
+@pytest.mark.parametrize("ions_turns", LARGE_HELICES)
+def test_large_active_block_residual_matches_oracle(ions_turns):
+    ni, nt = ions_turns
+    m = qb.Model.helix(N_ions=ni, N_turns=nt, hel_length=0.34 * nt, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                       lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
+                       dw=1.0, up=1.0, delta=0.04, order=2)
+    gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+    assert gs.nA == os_.nA == 2 * ni * nt
+    xg, xo = gs.initial_vector(0.2), os_.initial_vector(0.2)
+    assert rel(xg, xo) < 1e-12
+    x = xo + 1e-3 * np.random.default_rng(3).standard_normal(xo.size)
+    Fg, _ = gs.residual(0.2, x)
+    Fo, _ = os_.residual(0.2, x)
+    assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
+
+
 @pytest.mark.parametrize("single", [True, False])
 def test_device_broyden_matches_oracle_broyden(single):
     rng = np.random.default_rng(7)
