@@ -391,6 +391,153 @@ __global__ void __launch_bounds__(256, 2) sig2_invC(const cplx<T> *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------------
+// Persistent forms of kernels A and C for the power-of-two lengths N1 = 64..256 with 4 x 4
+// tiles (16 sequences a tile, 512 threads): one block per SM walks the tiles, and the
+// input values of the next tile are copied asynchronously into the second buffer while the
+// current tile is transformed, so the HBM reads overlap the transforms and the stores.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Kernel A: tile = 4 adjacent sequences x 4 adjacent m2; tiles ordered sequence-tile fastest
+template <int N1>
+__global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk, int n,
+                                                      const int2 *__restrict__ desc, int nY, FftPlan fp,
+                                                      const zc *__restrict__ tw, zc *__restrict__ Y, int nitems) {
+    constexpr int SA = 4, GA = 4, NS = SA * GA;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int nst = (nY + SA - 1) / SA;
+    const int m1max = (n + N2 - 1) / N2;  // zero padding beyond n energies
+    zc *buf0 = (zc *)smem_raw;
+    zc *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
+    zc *twc = twL + N1;            // W_Nf^{m2 l1} of the tile's four columns
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    auto load = [&](int it, zc *b) {
+        const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
+        for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
+            const int sl = t & 3, r = t >> 2, gl = r & 3, m1 = r >> 2;
+            const int s = s0 + sl, m2 = m20 + gl;
+            const int64_t w = (int64_t)N2 * m1 + m2;
+            zc *dst = b + (sl * GA + gl) * PL + pidx(m1);
+            if (m1 < m1max && s < nY && w < n) {
+                const int2 d = desc[s];
+                const double *blk = X + w * nblk;
+                if (d.x >= 0 && d.y == d.x + 1 && ((reinterpret_cast<uintptr_t>(blk + d.x) & 15) == 0)) {
+                    cp_async16(dst, blk + d.x);
+                } else {
+                    if (d.x >= 0) cp_async8(&dst->x, blk + d.x);
+                    else dst->x = 0.0;
+                    cp_async8(&dst->y, blk + d.y);
+                }
+            } else {
+                *dst = zc{0.0, 0.0};
+            }
+        }
+    };
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
+    if (blockIdx.x < nitems) load(blockIdx.x, buf0);
+    cp_async_commit();
+    int cur = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int nxt = it + gridDim.x;
+        if (nxt < nitems) load(nxt, buf0 + (cur ^ 1) * NS * PL);
+        cp_async_commit();
+        const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
+        for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
+            const int gl = t / N1, l1 = t % N1;
+            twc[t] = tw[(size_t)(m20 + gl) * l1];
+        }
+        cp_async_wait1();
+        __syncthreads();
+        zc *b = buf0 + cur * NS * PL;
+        for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), -1, twL);
+        __syncthreads();
+        for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
+            const int gl = t & 3, r = t >> 2, l1 = r % N1, sl = r / N1;
+            const int s = s0 + sl, m2 = m20 + gl;
+            if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * twc[gl * N1 + l1];
+        }
+        __syncthreads();  // the buffer and twc are rewritten by the next tiles
+        cur ^= 1;
+    }
+}
+
+// Kernel C: tile = one column jo+bb of a 2x2 output block x 4 adjacent m2; tiles ordered m2
+// fastest (neighbouring blocks read neighbouring 64-byte pieces of the same V rows)
+template <int N1>
+__global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, zc *__restrict__ SigR,
+                                                      zc *__restrict__ SigL, int nA, int nAs, int n,
+                                                      const double *__restrict__ Upair, FftPlan fp,
+                                                      const zc *__restrict__ tw, int nitems) {
+    constexpr int GC = 4, NS = 4 * GC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int nmt = N2 / GC, nfull = nA * nA;
+    const int m1max = (n + N2 - 1) / N2;
+    zc *buf0 = (zc *)smem_raw;
+    zc *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    auto tile = [&](int it, int &io, int &jo, int &bb, int &m20, double &c) {
+        const int pc = it / nmt;
+        m20 = (it % nmt) * GC;
+        bb = pc & 1;
+        const int pairid = pc >> 1, I = pairid % nAs, J = pairid / nAs;
+        io = 2 * I;
+        jo = 2 * J;
+        c = Upair[I + J * nAs];  // U_I U_J hbar^2 (delta/2pi)^2 / Nf, 0 if no interaction
+    };
+    auto load = [&](int it, zc *b) {
+        int io, jo, bb, m20;
+        double c;
+        tile(it, io, jo, bb, m20, c);
+        if (c == 0.0) return;  // src/self_energies.f90:167-171: a zero block, nothing to read
+        for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
+            const int gl = t & 3, r = t >> 2, sl = r & 3, l1 = r >> 2;
+            const int a = sl & 1, st = sl >> 1;
+            const size_t sid = (size_t)st * nfull + (io + a) + (size_t)(jo + bb) * nA;
+            cp_async16(b + (sl * GC + gl) * PL + pidx(l1), V + sid * Nf + (size_t)l1 * N2 + m20 + gl);
+        }
+    };
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
+    if (blockIdx.x < nitems) load(blockIdx.x, buf0);
+    cp_async_commit();
+    int cur = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int nxt = it + gridDim.x;
+        if (nxt < nitems) load(nxt, buf0 + (cur ^ 1) * NS * PL);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        int io, jo, bb, m20;
+        double c;
+        tile(it, io, jo, bb, m20, c);
+        zc *b = buf0 + cur * NS * PL;
+        if (c != 0.0)
+            for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), +1, twL);
+        __syncthreads();
+        for (int t = threadIdx.x; t < NS * m1max; t += blockDim.x) {
+            const int a = t & 1, st = (t >> 1) & 1, r = t >> 2;
+            const int gl = r & 3, m1 = r >> 2;
+            const int64_t w = (int64_t)N2 * m1 + m20 + gl;
+            if (w < n) {
+                zc v = (c != 0.0) ? b[((st * 2 + a) * GC + gl) * PL + pidx(m1)] : zc{0.0, 0.0};
+                zc *S = st ? SigL : SigR;
+                S[w * nfull + (io + a) + (size_t)(jo + bb) * nA] = zc{c * v.x, c * v.y};
+            }
+        }
+        __syncthreads();  // the buffer is rewritten by the next tiles
+        cur ^= 1;
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------
 static void factor_len(int L, FftLen &P) {
@@ -443,6 +590,29 @@ static InvCFn pick_invC(int N1, int GC) {
         }
     return sig2_invC<double, 0>;
 }
+
+using FwdAPFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, zc *, int);
+using InvCPFn = void (*)(const zc *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
+static FwdAPFn pick_fwdA_p(int N1) {
+    switch (N1) {
+        case 64: return sig2_fwdA_p<64>;
+        case 128: return sig2_fwdA_p<128>;
+        case 256: return sig2_fwdA_p<256>;
+    }
+    return nullptr;
+}
+static InvCPFn pick_invC_p(int N1) {
+    switch (N1) {
+        case 64: return sig2_invC_p<64>;
+        case 128: return sig2_invC_p<128>;
+        case 256: return sig2_invC_p<256>;
+    }
+    return nullptr;
+}
+static size_t smem_fwdA_p(int N1) { return sizeof(zc) * ((size_t)2 * 16 * padded_len(N1) + 5 * (size_t)N1); }
+static size_t smem_invC_p(int N1) { return sizeof(zc) * ((size_t)2 * 16 * padded_len(N1) + (size_t)N1); }
+// the persistent forms need N2 a multiple of the 4-column tile (true for N2 >= 64 here)
+static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p(fp.N1) && fp.N2 % 4 == 0; }
 
 int sigma2_setup(qs_handle *h) {
     const int n = h->n, nA = h->nA;
@@ -536,6 +706,12 @@ int sigma2_setup(qs_handle *h) {
     QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_mid(fp.N2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
     QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC(fp.N1, GC), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smC));
+    if (persistent_AC(fp)) {
+        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA_p(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_fwdA_p(fp.N1)));
+        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC_p(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_invC_p(fp.N1)));
+    }
     h->sig2_smem[0] = smA;
     h->sig2_smem[1] = smB;
     h->sig2_smem[2] = smC;
@@ -548,10 +724,17 @@ int sigma2_setup(qs_handle *h) {
 int sigma2_compute(qs_handle *h, const double *d_x) {
     const FftPlan &fp = h->fft;
     const int nA = h->nA;
-    dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
+    const bool pers = persistent_AC(fp);
     int pa = prof_begin(h, K_SIG2A);
-    pick_fwdA(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, h->sig2_smem[0], h->stream>>>(d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw,
-                                                             h->d_Y, h->sig2_SA, h->sig2_GA);
+    if (pers) {
+        const int nitems = (int)((h->nY + 3) / 4) * (fp.N2 / 4);
+        pick_fwdA_p(fp.N1)<<<std::min(nitems, 148), 512, smem_fwdA_p(fp.N1), h->stream>>>(
+            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, h->d_Y, nitems);
+    } else {
+        dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
+        pick_fwdA(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, h->sig2_smem[0], h->stream>>>(
+            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, h->d_Y, h->sig2_SA, h->sig2_GA);
+    }
     prof_end(h, pa);
     QS_CUDA(h, cudaGetLastError());
     if (h->sig2_npairs > 0) {
@@ -563,10 +746,16 @@ int sigma2_compute(qs_handle *h, const double *d_x) {
         prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
-    dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
     int pc = prof_begin(h, K_SIG2C);
-    pick_invC(fp.N1, h->sig2_GC)<<<gC, 256, h->sig2_smem[2], h->stream>>>(h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n,
-                                                             h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
+    if (pers) {
+        const int nitems = 2 * h->nAs * h->nAs * (fp.N2 / 4);
+        pick_invC_p(fp.N1)<<<std::min(nitems, 148), 512, smem_invC_p(fp.N1), h->stream>>>(
+            h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
+    } else {
+        dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
+        pick_invC(fp.N1, h->sig2_GC)<<<gC, 256, h->sig2_smem[2], h->stream>>>(
+            h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
+    }
     prof_end(h, pc);
     QS_CUDA(h, cudaGetLastError());
     return 0;
