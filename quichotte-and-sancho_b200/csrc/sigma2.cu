@@ -417,12 +417,13 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
     const int m1max = (n + N2 - 1) / N2;  // zero padding beyond n energies
     zc *buf0 = (zc *)smem_raw;
     zc *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
-    zc *twc = twL + N1;            // W_Nf^{m2 l1} of the tile's four columns
+    zc *twc = twL + N1;            // W_Nf^{m2 l1} of the tile's four columns, [l1][m2 - m20]
     for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
     auto load = [&](int it, zc *b) {
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
+        // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores)
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int sl = t & 3, r = t >> 2, gl = r & 3, m1 = r >> 2;
+            const int gl = t & 3, r = t >> 2, sl = r & 3, m1 = r >> 2;
             const int s = s0 + sl, m2 = m20 + gl;
             const int64_t w = (int64_t)N2 * m1 + m2;
             zc *dst = b + (sl * GA + gl) * PL + pidx(m1);
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
         cp_async_commit();
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
         for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
-            const int gl = t / N1, l1 = t % N1;
+            const int gl = t & 3, l1 = t >> 2;
             twc[t] = tw[(size_t)(m20 + gl) * l1];
         }
         cp_async_wait1();
@@ -459,10 +460,11 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
         zc *b = buf0 + cur * NS * PL;
         for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), -1, twL);
         __syncthreads();
+        // lanes: m2 fastest, then sequence, then l1
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int gl = t & 3, r = t >> 2, l1 = r % N1, sl = r / N1;
+            const int gl = t & 3, sl = (t >> 2) & 3, l1 = t >> 4;
             const int s = s0 + sl, m2 = m20 + gl;
-            if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * twc[gl * N1 + l1];
+            if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * twc[l1 * GA + gl];
         }
         __syncthreads();  // the buffer and twc are rewritten by the next tiles
         cur ^= 1;
@@ -522,9 +524,9 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, 
         if (c != 0.0)
             for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), +1, twL);
         __syncthreads();
+        // lanes: row a fastest (32-byte global runs), then m2, then stage (conflict-free reads)
         for (int t = threadIdx.x; t < NS * m1max; t += blockDim.x) {
-            const int a = t & 1, st = (t >> 1) & 1, r = t >> 2;
-            const int gl = r & 3, m1 = r >> 2;
+            const int a = t & 1, gl = (t >> 1) & 3, st = (t >> 3) & 1, m1 = t >> 4;
             const int64_t w = (int64_t)N2 * m1 + m20 + gl;
             if (w < n) {
                 zc v = (c != 0.0) ? b[((st * 2 + a) * GC + gl) * PL + pidx(m1)] : zc{0.0, 0.0};
