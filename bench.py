@@ -174,6 +174,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
     ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="both: the FP64 form, then the mixed form (headline value), with their ratio")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -192,58 +194,75 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
 
     m = model_cfg1(qb, args.n_omega)
-    solver = qb.Solver(m, device=local, alpha_mix=0.5, nhist=args.nhist, tolf=1e-6, maxscf=300, single_history=1)
     # this rank's block of the voltage sweep
     per = (len(VOLTS) + world - 1) // world
     block = VOLTS[rank * per:(rank + 1) * per] or VOLTS[-1:]
     seq = [block[k % len(block)] for k in range(args.warmup + args.steps)]
     fresh = [k == 0 or (k % len(block) == 0) for k in range(len(seq))]
-
     obs_bytes = 8 * (2 * m.Norb * m.Norb + m.Norb * m.n_omega + 2 * m.n_omega)
-    n_conv, iters = 0, []
-    prev_ok = False
-    for k in range(args.warmup):
-        # continuation as the reference's sweep: fresh after an unconverged voltage
-        r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
-        prev_ok = r["converged"]
-        solver.current(seq[k])
-        solver.observables()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    solver.profile(True)
-    l0 = qb.kernel_launches()
-    dev_s, wall0 = 0.0, time.perf_counter()
-    currents = []
-    for k in range(args.warmup, args.warmup + args.steps):
-        r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
-        prev_ok = r["converged"]
-        dev_s += r["seconds"]
-        n_conv += int(r["converged"])
-        iters.append(r["n_iter"])
-        currents.append(solver.current(seq[k]))
-        solver.observables()  # G_less_obs, dosd, trU, trD back to host buffers
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - wall0
-    launches = qb.kernel_launches() - l0
-    prof = solver.profile(False)
-    clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([dev_s, wall, float(n_conv)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
-        tc = t[2:].clone()
-        dist.all_reduce(tc, op=dist.ReduceOp.SUM)
-        dev_s, wall, n_conv = float(t[0]), float(t[1]), int(tc[0])
-        dist.barrier()
+
+    def run_arm(precision):
+        """warm-up + timed IV points of one solver form; the two forms do not fit in HBM
+        together, so each arm creates and releases its own solver"""
+        solver = qb.Solver(m, precision=precision, device=local, alpha_mix=0.5, nhist=args.nhist, tolf=1e-6,
+                           maxscf=300, single_history=1)
+        prev_ok = False
+        for k in range(args.warmup):
+            # continuation as the reference's sweep: fresh after an unconverged voltage
+            r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
+            prev_ok = r["converged"]
+            solver.current(seq[k])
+            solver.observables()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        solver.profile(True)
+        l0 = qb.kernel_launches()
+        dev_s, n_conv, iters, mixed_steps, currents = 0.0, 0, [], [], []
+        wall0 = time.perf_counter()
+        for k in range(args.warmup, args.warmup + args.steps):
+            r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
+            prev_ok = r["converged"]
+            dev_s += r["seconds"]
+            n_conv += int(r["converged"])
+            iters.append(r["n_iter"])
+            mixed_steps.append(r["n_mixed"])
+            currents.append(solver.current(seq[k]))
+            solver.observables()  # G_less_obs, dosd, trU, trD back to host buffers
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        out = dict(launches=qb.kernel_launches() - l0, prof=solver.profile(False), clk=clocks.stop(), iters=iters,
+                   mixed_steps=mixed_steps, currents=currents, nA=solver.nA, Nf=solver.Nf, n_vec=solver.n_vec)
+        solver.close()
+        if world > 1:
+            t = torch.tensor([dev_s, wall, float(n_conv)], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
+            tc = t[2:].clone()
+            dist.all_reduce(tc, op=dist.ReduceOp.SUM)
+            dev_s, wall, n_conv = float(t[0]), float(t[1]), int(tc[0])
+            dist.barrier()
+        out.update(dev_s=dev_s, wall=wall, n_conv=n_conv, value=n_conv / dev_s if dev_s > 0 else 0.0,
+                   e2e=n_conv / wall if wall > 0 else 0.0)
+        return out
+
+    arms = {}
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+        arms[prec] = run_arm(qb.QS_PREC_MIXED if prec == "mixed" else qb.QS_PREC_FP64)
+    head = arms.get("mixed") or arms["fp64"]
+    f64 = arms.get("fp64")
+    dev_s, wall, n_conv = head["dev_s"], head["wall"], head["n_conv"]
+    launches, clk, iters = head["launches"], head["clk"], head["iters"]
+    prof = (f64 or head)["prof"]
     if rank == 0:
         points = args.steps * world
         peaks, src = measured_peaks()
-        # roofline of the dominant kernel (largest device time): algorithmic work per launch
-        N, nA, n = m.Norb, solver.nA, m.n_omega
+        # roofline of the dominant kernel of the FP64 form (largest device time):
+        # algorithmic work per launch
+        N, nA, n = m.Norb, head["nA"], m.n_omega
         fam, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
-        nY, Nf, nvec = nA * nA + nA * (nA + 1) // 2, solver.Nf, solver.n_vec
+        nY, Nf, nvec = nA * nA + nA * (nA + 1) // 2, head["Nf"], head["n_vec"]
         nh = args.nhist
         work = {  # algorithmic FLOPs (FP64 compute-bound kernels) or bytes (HBM-bound) per launch
             "dyson_gj": ("fp64", n * 8.0 * N ** 3),                       # G^r: N^3 complex MACs per energy
@@ -266,13 +285,14 @@ def main():
             roof = {"kernel": fam, "bound": kind, "achieved": achieved, "peak": peak, "unit": unit,
                     "frac": achieved / peak, "traffic": None, "peak_source": src_note,
                     "per_launch_work": per_launch, "launches": cnt, "avg_launch_ms": ms / cnt}
+        prec_name = "mixed" if "mixed" in arms else "fp64"
         line = {
             "metric": "converged IV points/s", "value": n_conv / dev_s if dev_s > 0 else 0.0,
             "unit": "IV points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32+f64" if prec_name == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": f"helix 10x6 (120x120 complex), {n} energies on [-12,12] eV, order 2, U=1.0 eV, "
-                                   "V sweep -1..1 V step 0.05 with continuation", "precision": "fp64", "nhist": args.nhist,
+                                   "V sweep -1..1 V step 0.05 with continuation", "precision": prec_name, "nhist": args.nhist,
                        "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 (no flush needed)",
                        "scf_steps_per_point": iters, "converged_points": n_conv},
             "e2e": {"value": n_conv / wall if wall > 0 else 0.0, "unit": "IV points/s", "h2d_bytes_per_step": 8,
@@ -281,12 +301,24 @@ def main():
             "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
             "roofline": roof,
             "clocks": clk,
-            "currents_A": [list(c) for c in currents],
+            "currents_A": [list(c) for c in head["currents"]],
         }
+        if "mixed" in arms:
+            line["config"]["mixed"] = ("Sigma2 FFTs, 2x2 algebra and spectra in FP32 while max|F| > max(1e-5, 100 tolf) "
+                                       "(the FP32 noise floor is ~1e-5); then FP64 steps until an FP64 residual meets "
+                                       "tolf; Dyson/Keldysh, Broyden and observables FP64")
+            line["config"]["fp32_steps_per_point"] = head["mixed_steps"]
+        if f64 is not None and "mixed" in arms:
+            j64, jmx = np.array(f64["currents"]), np.array(head["currents"])
+            line["fp64"] = {"value": f64["value"], "e2e": f64["e2e"], "ms_per_step": 1000.0 * f64["dev_s"] / args.steps,
+                            "scf_steps_per_point": f64["iters"], "kernel_ms": {k: round(v[0], 3) for k, v in
+                                                                               f64["prof"].items() if v[1]}}
+            line["mixed_over_fp64"] = head["value"] / f64["value"] if f64["value"] > 0 else None
+            line["current_rel_err_vs_fp64"] = float(np.max(np.abs(jmx - j64)) / np.max(np.abs(j64)))
+            line["kernel_ms_mixed"] = {k: round(v[0], 3) for k, v in head["prof"].items() if v[1]}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.ref_sample)
         print(json.dumps(line), flush=True)
-    solver.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

@@ -64,6 +64,8 @@ typedef struct qs_scf_result {
     qs_scf_step *log; /* caller buffer for the scf_V_<V>.dat lines, or NULL     */
     int log_cap, n_log;
     double seconds; /* device time of the solve                                 */
+    int n_mixed;    /* QS_PREC_MIXED: leading steps whose residual used the FP32
+                     * self-energies; the later steps, convergence included, are FP64 */
 } qs_scf_result;
 
 typedef struct qs_handle qs_handle;
@@ -103,7 +105,8 @@ int qs_residual(qs_handle *h, double Volt, const double *x, double *F, int *abor
 
 /* unpack_gf + equal_time_lesser + sigma_first_order + sigma2_compute(.true.)
  * (src/self_energies.f90:45-72,135-219): Sigma2^r, Sigma2^< as (nA,nA,n_omega) complex
- * column-major, and Sigma1 (Norb*Norb complex); any output may be NULL. */
+ * column-major, and Sigma1 (Norb*Norb complex); any output may be NULL. On a QS_PREC_MIXED
+ * handle Sigma2 is formed as in the FP32 phase of its solves (FP32 transforms). */
 int qs_self_energies(qs_handle *h, const double *x, double *SigR2, double *SigL2, double *Sig1);
 
 /* invert_complex (common/linear_algebra.f90:58-88) over a batch: A holds `batch`

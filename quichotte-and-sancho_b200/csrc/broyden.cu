@@ -412,6 +412,22 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
     return 0;
 }
 
+int vec_maxabs(qs_handle *h, const double *d_v, int64_t n, double &mx) {
+    const int nb = red_blocks(n);
+    double *part = h->d_red, *fin = h->d_red + (size_t)RED_BLOCKS * 2 * MAXH;
+    int pi = prof_begin(h, K_BROYDEN);
+    vec_norms<<<nb, RED_THREADS, 0, h->stream>>>(d_v, nullptr, n, part);
+    prof_end(h, pi);
+    count_launch();
+    part_reduce<<<1, 32, 0, h->stream>>>(part, nb, 3, 3, 1, fin);
+    QS_CUDA(h, cudaGetLastError());
+    double hv[3];
+    QS_CUDA(h, cudaMemcpyAsync(hv, fin, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QS_CUDA(h, cudaStreamSynchronize(h->stream));
+    mx = hv[0];
+    return 0;
+}
+
 size_t broyden_red_len() { return (size_t)RED_BLOCKS * 2 * MAXH + 4 * MAXH; }
 
 }  // namespace qs

@@ -139,6 +139,7 @@ struct qs_handle {
     int Norb = 0, N_sites = 0, N_atoms = 0, order = 0, n = 0, device = 0, precision = 0;
     double mu = 0, beta = 0, delta = 0, alpha_mix = 0.5, tolf = 1e-6, tolf_order1 = 1e-8;
     int nhist = 16, maxscf = 300;
+    double mixed_switch = 1e-4;  // QS_PREC_MIXED: FP32 max|F| below which the residual turns FP64
     bool single = true;
     std::vector<double> H, GammaL, GammaR, U_site, omega;  // complex arrays as double pairs
     std::vector<int> atom_norb, atom_first;
@@ -168,7 +169,6 @@ struct qs_handle {
     double *sig2_Upair = nullptr;  // U_I U_J hbar^2 (delta/2pi)^2 / Nf per site pair
     int2 *sig2_pairs = nullptr;    // interacting site pairs I <= J
     int sig2_npairs = 0, sig2_SA = 1, sig2_GA = 1, sig2_GC = 1;
-    size_t sig2_smem[3] = {0, 0, 0};
     // sweep scratch
     qs::zc *d_G = nullptr;  // Dyson output (G_AA for all energies, or full G for a chunk)
     size_t G_chunk = 0;     // energies per chunk in full-G mode
@@ -216,7 +216,10 @@ void prof_end(qs_handle *h, int idx);
 
 // launchers (implemented in the .cu files)
 int sigma2_setup(qs_handle *h);
-int sigma2_compute(qs_handle *h, const double *d_x);
+// fp32: FFTs, 2x2 algebra and spectra in FP32 (QS_PREC_MIXED handles), Sigma written in FP64
+int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
+// max |v_i| over a device vector (uses the Broyden reduction scratch)
+int vec_maxabs(qs_handle *h, const double *d_v, int64_t n, double &mx);
 int equal_time_lesser_sigma1(qs_handle *h, const double *d_x);
 enum SweepMode { M_INIT2 = 1, M_SCF2 = 2, M_SCF1 = 3, M_FINAL = 4 };
 int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x);

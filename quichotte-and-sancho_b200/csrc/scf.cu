@@ -267,20 +267,51 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
     return 0;
 }
 
+// The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: the leading steps form the
+// second-order self-energies in FP32 (FFTs, 2x2 algebra and spectra); once max|F| falls
+// below mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the step is
+// redone and the solve continues in FP64. The FP32 self-energies leave a noise floor of
+// about 1e-5 in F on the 120x120 helix, so FP32 steps stop well above it. Convergence
+// (max|F| < tolf) is always judged on an FP64 residual, and the converged state meets the
+// FP64 solve's criterion.
 struct Residual2 : BroydenResidual {
     qs_handle *h;
     double V;
     int iter = 0;
-    int operator()(const double *d_x, double *d_F, bool &abort) override {
-        iter++;
+    bool fp32 = false;  // this solve is still in its FP32 phase
+    int n_mixed = 0;
+    double best = HUGE_VAL;
+    int since_best = 0;
+    int eval(const double *d_x, double *d_F, bool &abort, bool use32) {
         int rc;
         if ((rc = equal_time_lesser_sigma1(h, d_x))) return rc;
-        if ((rc = sigma2_compute(h, d_x))) return rc;
+        if ((rc = sigma2_compute(h, d_x, use32))) return rc;
         if ((rc = sweep(h, M_SCF2, V, true, d_F, d_x))) return rc;
         SanityOut s;
         if ((rc = sweep_sanity(h, s))) return rc;
         abort = s.runaway;
         if (abort) QS_CUDA(h, cudaMemsetAsync(d_F, 0, sizeof(double) * h->n_vec, h->stream));
+        return 0;
+    }
+    int operator()(const double *d_x, double *d_F, bool &abort) override {
+        iter++;
+        int rc;
+        if (!fp32) return eval(d_x, d_F, abort, false);
+        if ((rc = eval(d_x, d_F, abort, true))) return rc;
+        if (abort) return 0;
+        double fmax;
+        if ((rc = vec_maxabs(h, d_F, h->n_vec, fmax))) return rc;
+        if (fmax < best) {
+            best = fmax;
+            since_best = 0;
+        } else {
+            since_best++;
+        }
+        if (fmax < h->mixed_switch || since_best >= 5 || iter >= h->maxscf / 2) {
+            fp32 = false;  // redo this step in FP64
+            return eval(d_x, d_F, abort, false);
+        }
+        n_mixed++;
         return 0;
     }
 };
@@ -468,6 +499,7 @@ int qs_create(const qs_problem *p, qs_handle **out) {
     h->alpha_mix = p->alpha_mix;
     h->tolf = p->tolf;
     h->tolf_order1 = p->tolf_order1;
+    h->mixed_switch = std::max(1e-5, 100.0 * p->tolf);
     h->nhist = p->nhist;
     h->maxscf = p->maxscf;
     h->single = p->single_history != 0;
@@ -484,8 +516,8 @@ int qs_create(const qs_problem *p, qs_handle **out) {
         h->err = "qs_create: need 2 <= Norb <= 512 and n_omega >= 1";
         return -1;
     }
-    if (h->precision != QS_PREC_FP64) {
-        h->err = "qs_create: only QS_PREC_FP64 is available in this build";
+    if (h->precision != QS_PREC_FP64 && h->precision != QS_PREC_MIXED) {
+        h->err = "qs_create: precision must be QS_PREC_FP64 or QS_PREC_MIXED";
         return -1;
     }
     if (h->nhist > 32 || h->nhist < 0) {
@@ -655,17 +687,19 @@ int qs_solve_scf(qs_handle *h, double Volt, int fresh_start, qs_scf_result *res)
     QS_CUDA(h, cudaSetDevice(h->device));
     QS_CUDA(h, cudaEventRecord(h->ev0, h->stream));
     BroydenOut bo;
-    int rc = 0;
+    int rc = 0, n_mixed = 0;
     bool fresh = fresh_start || !h->have_x;
     if (h->order == 2) {
         if (fresh && (rc = sweep(h, M_INIT2, Volt, false, h->d_x, nullptr))) return rc;
         Residual2 r;
         r.h = h;
         r.V = Volt;
+        r.fp32 = (h->precision == QS_PREC_MIXED);
         rc = broyden_solve_dev(h, r, h->d_x, h->d_F, h->d_Fold, h->d_xold, h->d_hdF, h->d_hU, h->n_vec, h->alpha_mix,
                                h->nhist, h->maxscf, h->tolf, h->single, bo);
         if (rc) return rc;
         h->have_x = true;
+        n_mixed = r.n_mixed;
     } else if (h->order == 1) {
         if (fresh) {
             // G^<(t=0) of the non-interacting system (src/scf.f90:103-108)
@@ -716,6 +750,7 @@ int qs_solve_scf(qs_handle *h, double Volt, int fresh_start, qs_scf_result *res)
     for (auto &e : bo.log)
         if (res->log && res->n_log < res->log_cap) res->log[res->n_log++] = e;
     res->seconds = ms * 1e-3;
+    res->n_mixed = n_mixed;
     return 0;
 }
 
@@ -803,7 +838,7 @@ int qs_self_energies(qs_handle *h, const double *x, double *SigR2, double *SigL2
     QS_CUDA(h, cudaMemcpyAsync(h->d_F, x, sizeof(double) * h->n_vec, cudaMemcpyHostToDevice, h->stream));
     if ((rc = convert_ref_to_dl(h->stream, h->nA, h->n, h->d_F, h->d_x))) return -rc;
     if ((rc = equal_time_lesser_sigma1(h, h->d_x))) return rc;
-    if ((rc = sigma2_compute(h, h->d_x))) return rc;
+    if ((rc = sigma2_compute(h, h->d_x, h->precision == QS_PREC_MIXED))) return rc;
     const size_t bytes = sizeof(zc) * (size_t)h->n * h->nA * h->nA;
     if (SigR2) QS_CUDA(h, cudaMemcpyAsync(SigR2, h->d_SigR, bytes, cudaMemcpyDeviceToHost, h->stream));
     if (SigL2) QS_CUDA(h, cudaMemcpyAsync(SigL2, h->d_SigL, bytes, cudaMemcpyDeviceToHost, h->stream));

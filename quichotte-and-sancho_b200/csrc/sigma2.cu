@@ -26,6 +26,9 @@
 
 namespace qs {
 
+// an FP64 twiddle at the kernel's element type
+template <typename T> __device__ __forceinline__ cplx<T> cvt(zc v) { return cplx<T>{(T)v.x, (T)v.y}; }
+
 // ---------------------------------------------------------------------------------
 // Kernel A: forward length-N1 transforms of the zero-padded element sequences.
 // Block tile: SA adjacent sequences x GA adjacent m2 (SA*16 B contiguous per energy block
@@ -36,7 +39,7 @@ namespace qs {
 template <typename T, int N1C>
 __global__ void __launch_bounds__(256, 2) sig2_fwdA(const double *__restrict__ X, int64_t nblk, int n,
                                                  const int2 *__restrict__ desc, int nY, FftPlan fp,
-                                                 const cplx<T> *__restrict__ tw, cplx<T> *__restrict__ Y, int SA_rt,
+                                                 const zc *__restrict__ tw, cplx<T> *__restrict__ Y, int SA_rt,
                                                  int GA_rt) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N1 = N1C ? N1C : fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
@@ -46,7 +49,7 @@ __global__ void __launch_bounds__(256, 2) sig2_fwdA(const double *__restrict__ X
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
     cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
     // only m1 < ceil((n - m2)/N2) can be non-zero (zero padding beyond n energies)
     const int m1max = (n + N2 - 1) / N2;
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(256, 2) sig2_fwdA(const double *__restrict__ X
         int l1 = r % N1, sl = r / N1;
         int s = s0 + sl, m2 = m20 + gl;
         if (s < nY && m2 < N2) {
-            cplx<T> v = buf[(sl * GA + gl) * PL + pidx(l1)] * tw[m2 * l1];
+            cplx<T> v = buf[(sl * GA + gl) * PL + pidx(l1)] * cvt<T>(tw[m2 * l1]);
             Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = v;
         }
     }
@@ -196,7 +199,7 @@ __device__ __forceinline__ void mid_load(const cplx<T> *__restrict__ Y, cplx<T> 
 template <typename T, int N2C>
 __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, cplx<T> *__restrict__ V,
                                                 const int2 *__restrict__ pairs, int nA, FftPlan fp,
-                                                const cplx<T> *__restrict__ tw, int nitems) {
+                                                const zc *__restrict__ tw, int nitems) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N1 = fp.N1, N2 = N2C ? N2C : fp.N2, Nf = fp.Nf, PL = padded_len(N2);
     const int ncp = N1 / 2 + 1;
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, c
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     cplx<T> *twL = O + (32 + nw) * PL;  // W_N2^m, m < N2
     cplx<T> *twc = twL + N2;            // W_Nf^{m2 col} of the item's two columns
-    for (int m = threadIdx.x; m < N2; m += blockDim.x) twL[m] = tw[(size_t)m * N1];
+    for (int m = threadIdx.x; m < N2; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N1]);
     const int G = fft_group(N2);
 
     if (blockIdx.x < nitems) mid_load<T, N2C>(Y, S0, blockIdx.x, ncp, pairs, nA, fp, PL);
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, c
         const bool diag = (I == J);
         const int nblko = diag ? 1 : 2;
         for (int t = threadIdx.x; t < 2 * N2; t += blockDim.x)  // used after two barriers
-            twc[t] = tw[(size_t)(t % N2) * ((t < N2) ? c : cp)];
+            twc[t] = cvt<T>(tw[(size_t)(t % N2) * ((t < N2) ? c : cp)]);
 
         for (int q = warp * G; q < ncols * 12; q += nw * G)
             warp_fft_group(S + q * PL, PL, min(G, ncols * 12 - q), scr, fp.p2, -1, twL);
@@ -328,7 +331,7 @@ template <typename T, int N1C>
 __global__ void __launch_bounds__(256, 2) sig2_invC(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
                                                  zc *__restrict__ SigL, int nA, int nAs, int n,
                                                  const double *__restrict__ Upair, FftPlan fp,
-                                                 const cplx<T> *__restrict__ tw, int GC_rt) {
+                                                 const zc *__restrict__ tw, int GC_rt) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N1 = N1C ? N1C : fp.N1, N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int GC = N1C ? 4 : GC_rt;
@@ -357,7 +360,7 @@ __global__ void __launch_bounds__(256, 2) sig2_invC(const cplx<T> *__restrict__ 
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
     cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GC, r = t / GC;
         int sl = r % 4, l1 = r / 4;
@@ -405,20 +408,24 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Kernel A: tile = 4 adjacent sequences x 4 adjacent m2; tiles ordered sequence-tile fastest
-template <int N1>
+// Kernel A: tile = 4 adjacent sequences x 4 adjacent m2; tiles ordered sequence-tile fastest.
+// The FP64 values are copied into a staging buffer; with T = float they are converted into
+// a work buffer before the transforms (Y then holds FP32 spectra).
+template <typename T, int N1>
 __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk, int n,
                                                       const int2 *__restrict__ desc, int nY, FftPlan fp,
-                                                      const zc *__restrict__ tw, zc *__restrict__ Y, int nitems) {
+                                                      const zc *__restrict__ tw, cplx<T> *__restrict__ Y, int nitems) {
     constexpr int SA = 4, GA = 4, NS = SA * GA;
+    constexpr bool F64 = sizeof(T) == 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int nst = (nY + SA - 1) / SA;
     const int m1max = (n + N2 - 1) / N2;  // zero padding beyond n energies
-    zc *buf0 = (zc *)smem_raw;
-    zc *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
-    zc *twc = twL + N1;            // W_Nf^{m2 l1} of the tile's four columns, [l1][m2 - m20]
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    zc *stg0 = (zc *)smem_raw;                                          // 2 x NS staging sequences
+    cplx<T> *wb = F64 ? nullptr : (cplx<T> *)(stg0 + 2 * NS * PL);     // FP32 work sequences
+    cplx<T> *twL = F64 ? (cplx<T> *)(stg0 + 2 * NS * PL) : wb + NS * PL;  // W_N1^m, m < N1
+    cplx<T> *twc = twL + N1;  // W_Nf^{m2 l1} of the tile's four columns, [l1][m2 - m20]
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
     auto load = [&](int it, zc *b) {
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
         // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores)
@@ -443,22 +450,30 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
         }
     };
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
-    if (blockIdx.x < nitems) load(blockIdx.x, buf0);
+    if (blockIdx.x < nitems) load(blockIdx.x, stg0);
     cp_async_commit();
     int cur = 0;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int nxt = it + gridDim.x;
-        if (nxt < nitems) load(nxt, buf0 + (cur ^ 1) * NS * PL);
+        if (nxt < nitems) load(nxt, stg0 + (cur ^ 1) * NS * PL);
         cp_async_commit();
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
         for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
             const int gl = t & 3, l1 = t >> 2;
-            twc[t] = tw[(size_t)(m20 + gl) * l1];
+            twc[t] = cvt<T>(tw[(size_t)(m20 + gl) * l1]);
         }
         cp_async_wait1();
         __syncthreads();
-        zc *b = buf0 + cur * NS * PL;
-        for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), -1, twL);
+        cplx<T> *b;
+        if constexpr (F64) {
+            b = stg0 + cur * NS * PL;
+        } else {
+            const zc *sb = stg0 + cur * NS * PL;
+            for (int t = threadIdx.x; t < NS * PL; t += blockDim.x) wb[t] = cvt<T>(sb[t]);
+            __syncthreads();
+            b = wb;
+        }
+        for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<T, N1>(b + q * PL, PL, min(G, NS - q), -1, twL);
         __syncthreads();
         // lanes: m2 fastest, then sequence, then l1
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
@@ -466,15 +481,15 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
             const int s = s0 + sl, m2 = m20 + gl;
             if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * twc[l1 * GA + gl];
         }
-        __syncthreads();  // the buffer and twc are rewritten by the next tiles
+        __syncthreads();  // the buffers and twc are rewritten by the next tiles
         cur ^= 1;
     }
 }
 
 // Kernel C: tile = one column jo+bb of a 2x2 output block x 4 adjacent m2; tiles ordered m2
 // fastest (neighbouring blocks read neighbouring 64-byte pieces of the same V rows)
-template <int N1>
-__global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, zc *__restrict__ SigR,
+template <typename T, int N1>
+__global__ void __launch_bounds__(512, 1) sig2_invC_p(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
                                                       zc *__restrict__ SigL, int nA, int nAs, int n,
                                                       const double *__restrict__ Upair, FftPlan fp,
                                                       const zc *__restrict__ tw, int nitems) {
@@ -483,9 +498,9 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, 
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int nmt = N2 / GC, nfull = nA * nA;
     const int m1max = (n + N2 - 1) / N2;
-    zc *buf0 = (zc *)smem_raw;
-    zc *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = tw[(size_t)m * N2];
+    cplx<T> *buf0 = (cplx<T> *)smem_raw;
+    cplx<T> *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
+    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
     auto tile = [&](int it, int &io, int &jo, int &bb, int &m20, double &c) {
         const int pc = it / nmt;
         m20 = (it % nmt) * GC;
@@ -495,7 +510,7 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, 
         jo = 2 * J;
         c = Upair[I + J * nAs];  // U_I U_J hbar^2 (delta/2pi)^2 / Nf, 0 if no interaction
     };
-    auto load = [&](int it, zc *b) {
+    auto load = [&](int it, cplx<T> *b) {
         int io, jo, bb, m20;
         double c;
         tile(it, io, jo, bb, m20, c);
@@ -504,7 +519,7 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, 
             const int gl = t & 3, r = t >> 2, sl = r & 3, l1 = r >> 2;
             const int a = sl & 1, st = sl >> 1;
             const size_t sid = (size_t)st * nfull + (io + a) + (size_t)(jo + bb) * nA;
-            cp_async16(b + (sl * GC + gl) * PL + pidx(l1), V + sid * Nf + (size_t)l1 * N2 + m20 + gl);
+            cp_async_elem(b + (sl * GC + gl) * PL + pidx(l1), V + sid * Nf + (size_t)l1 * N2 + m20 + gl, true);
         }
     };
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
@@ -520,18 +535,18 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const zc *__restrict__ V, 
         int io, jo, bb, m20;
         double c;
         tile(it, io, jo, bb, m20, c);
-        zc *b = buf0 + cur * NS * PL;
+        cplx<T> *b = buf0 + cur * NS * PL;
         if (c != 0.0)
-            for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<double, N1>(b + q * PL, PL, min(G, NS - q), +1, twL);
+            for (int q = warp * G; q < NS; q += nw * G) warp_fft_pow2<T, N1>(b + q * PL, PL, min(G, NS - q), +1, twL);
         __syncthreads();
         // lanes: row a fastest (32-byte global runs), then m2, then stage (conflict-free reads)
         for (int t = threadIdx.x; t < NS * m1max; t += blockDim.x) {
             const int a = t & 1, gl = (t >> 1) & 3, st = (t >> 3) & 1, m1 = t >> 4;
             const int64_t w = (int64_t)N2 * m1 + m20 + gl;
             if (w < n) {
-                zc v = (c != 0.0) ? b[((st * 2 + a) * GC + gl) * PL + pidx(m1)] : zc{0.0, 0.0};
+                cplx<T> v = (c != 0.0) ? b[((st * 2 + a) * GC + gl) * PL + pidx(m1)] : cplx<T>{0, 0};
                 zc *S = st ? SigL : SigR;
-                S[w * nfull + (io + a) + (size_t)(jo + bb) * nA] = zc{c * v.x, c * v.y};
+                S[w * nfull + (io + a) + (size_t)(jo + bb) * nA] = zc{c * (double)v.x, c * (double)v.y};
             }
         }
         __syncthreads();  // the buffer is rewritten by the next tiles
@@ -565,56 +580,92 @@ static int good_fft_size(int nmin) {
     }
 }
 
-// the kernel instantiations for a plan: compile-time lengths for the power-of-two splits
-using FwdAFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, zc *, int, int);
-using MidFn = void (*)(const zc *, zc *, const int2 *, int, FftPlan, const zc *, int);
-using InvCFn = void (*)(const zc *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
-static FwdAFn pick_fwdA(int N1, int SA, int GA) {
-    if (SA == 4 && GA == 4) switch (N1) {
-            case 64: return sig2_fwdA<double, 64>;
-            case 128: return sig2_fwdA<double, 128>;
-            case 256: return sig2_fwdA<double, 256>;
-        }
-    return sig2_fwdA<double, 0>;
-}
-static MidFn pick_mid(int N2) {
-    switch (N2) {
-        case 64: return sig2_mid<double, 64>;
-        case 128: return sig2_mid<double, 128>;
-    }
-    return sig2_mid<double, 0>;
-}
-static InvCFn pick_invC(int N1, int GC) {
-    if (GC == 4) switch (N1) {
-            case 64: return sig2_invC<double, 64>;
-            case 128: return sig2_invC<double, 128>;
-            case 256: return sig2_invC<double, 256>;
-        }
-    return sig2_invC<double, 0>;
-}
+// the kernel instantiations for a plan and element type: compile-time lengths for the
+// power-of-two splits, persistent forms of kernels A and C for those
+template <typename T>
+using FwdAFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, cplx<T> *, int, int);
+template <typename T> using MidFn = void (*)(const cplx<T> *, cplx<T> *, const int2 *, int, FftPlan, const zc *, int);
+template <typename T>
+using InvCFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
+template <typename T>
+using FwdAPFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, cplx<T> *, int);
+template <typename T>
+using InvCPFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
 
-using FwdAPFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, zc *, int);
-using InvCPFn = void (*)(const zc *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
-static FwdAPFn pick_fwdA_p(int N1) {
+template <typename T> static FwdAFn<T> pick_fwdA(int N1, int SA, int GA) {
+    if (SA == 4 && GA == 4) switch (N1) {
+            case 64: return sig2_fwdA<T, 64>;
+            case 128: return sig2_fwdA<T, 128>;
+            case 256: return sig2_fwdA<T, 256>;
+        }
+    return sig2_fwdA<T, 0>;
+}
+template <typename T> static MidFn<T> pick_mid(int N2) {
+    switch (N2) {
+        case 64: return sig2_mid<T, 64>;
+        case 128: return sig2_mid<T, 128>;
+    }
+    return sig2_mid<T, 0>;
+}
+template <typename T> static InvCFn<T> pick_invC(int N1, int GC) {
+    if (GC == 4) switch (N1) {
+            case 64: return sig2_invC<T, 64>;
+            case 128: return sig2_invC<T, 128>;
+            case 256: return sig2_invC<T, 256>;
+        }
+    return sig2_invC<T, 0>;
+}
+template <typename T> static FwdAPFn<T> pick_fwdA_p(int N1) {
     switch (N1) {
-        case 64: return sig2_fwdA_p<64>;
-        case 128: return sig2_fwdA_p<128>;
-        case 256: return sig2_fwdA_p<256>;
+        case 64: return sig2_fwdA_p<T, 64>;
+        case 128: return sig2_fwdA_p<T, 128>;
+        case 256: return sig2_fwdA_p<T, 256>;
     }
     return nullptr;
 }
-static InvCPFn pick_invC_p(int N1) {
+template <typename T> static InvCPFn<T> pick_invC_p(int N1) {
     switch (N1) {
-        case 64: return sig2_invC_p<64>;
-        case 128: return sig2_invC_p<128>;
-        case 256: return sig2_invC_p<256>;
+        case 64: return sig2_invC_p<T, 64>;
+        case 128: return sig2_invC_p<T, 128>;
+        case 256: return sig2_invC_p<T, 256>;
     }
     return nullptr;
 }
-static size_t smem_fwdA_p(int N1) { return sizeof(zc) * ((size_t)2 * 16 * padded_len(N1) + 5 * (size_t)N1); }
-static size_t smem_invC_p(int N1) { return sizeof(zc) * ((size_t)2 * 16 * padded_len(N1) + (size_t)N1); }
+template <typename T> static size_t smem_fwdA_p(int N1) {
+    const size_t PL = padded_len(N1);
+    return sizeof(zc) * 2 * 16 * PL + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * 16 * PL) + sizeof(cplx<T>) * 5 * N1;
+}
+template <typename T> static size_t smem_invC_p(int N1) {
+    return sizeof(cplx<T>) * ((size_t)2 * 16 * padded_len(N1) + (size_t)N1);
+}
+template <typename T> static size_t smem_A(const qs_handle *h) {
+    return sizeof(cplx<T>) * ((size_t)(h->sig2_SA * h->sig2_GA + 8) * padded_len(h->fft.N1) + h->fft.N1);
+}
+template <typename T> static size_t smem_B(const qs_handle *h) {
+    return sizeof(cplx<T>) * ((size_t)(2 * 24 + 32 + 16) * padded_len(h->fft.N2) + 3 * h->fft.N2);
+}
+template <typename T> static size_t smem_C(const qs_handle *h) {
+    return sizeof(cplx<T>) * ((size_t)(4 * h->sig2_GC + 8) * padded_len(h->fft.N1) + h->fft.N1);
+}
 // the persistent forms need N2 a multiple of the 4-column tile (true for N2 >= 64 here)
-static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p(fp.N1) && fp.N2 % 4 == 0; }
+static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p<double>(fp.N1) && fp.N2 % 4 == 0; }
+
+template <typename T> static int sigma2_attributes(qs_handle *h) {
+    const FftPlan &fp = h->fft;
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_A<T>(h)));
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_mid<T>(fp.N2), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_B<T>(h)));
+    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC<T>(fp.N1, h->sig2_GC),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_C<T>(h)));
+    if (persistent_AC(fp)) {
+        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA_p<T>(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_fwdA_p<T>(fp.N1)));
+        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC_p<T>(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_invC_p<T>(fp.N1)));
+    }
+    return 0;
+}
 
 int sigma2_setup(qs_handle *h) {
     const int n = h->n, nA = h->nA;
@@ -687,55 +738,42 @@ int sigma2_setup(qs_handle *h) {
         h->err = "sigma2: FFT length " + std::to_string(fp.Nf) + " needs N1 <= 512 and N2 <= 128";
         return -1;
     }
-    const int PL1 = padded_len(fp.N1), PL2 = padded_len(fp.N2);
+    const int PL1 = padded_len(fp.N1);
     int GA = std::min(fp.N2, 4), SA = 4;
     while ((size_t)(SA * GA + 8) * PL1 * sizeof(zc) > 112 * 1024 && GA > 1) GA /= 2;
     while ((size_t)(SA * GA + 8) * PL1 * sizeof(zc) > 112 * 1024 && SA > 1) SA /= 2;
-    h->sig2_SA = SA;
-    h->sig2_GA = GA;
     int GC = std::min(fp.N2, 4);
     while ((size_t)(4 * GC + 8) * PL1 * sizeof(zc) > 112 * 1024 && GC > 1) GC /= 2;
+    h->sig2_SA = SA;
+    h->sig2_GA = GA;
     h->sig2_GC = GC;
-    size_t smA = sizeof(zc) * ((size_t)(SA * GA + 8) * PL1 + fp.N1);
-    size_t smB = sizeof(zc) * ((size_t)(2 * 24 + 32 + 16) * PL2 + 3 * fp.N2);
-    size_t smC = sizeof(zc) * ((size_t)(4 * GC + 8) * PL1 + fp.N1);
-    if (smA > SMEM_MAX || smB > SMEM_MAX || smC > SMEM_MAX) {
+    if (smem_A<double>(h) > SMEM_MAX || smem_B<double>(h) > SMEM_MAX || smem_C<double>(h) > SMEM_MAX) {
         h->err = "sigma2: FFT tiles exceed shared memory";
         return -1;
     }
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA(fp.N1, SA, GA), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smA));
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_mid(fp.N2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC(fp.N1, GC), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smC));
-    if (persistent_AC(fp)) {
-        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA_p(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_fwdA_p(fp.N1)));
-        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC_p(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_invC_p(fp.N1)));
-    }
-    h->sig2_smem[0] = smA;
-    h->sig2_smem[1] = smB;
-    h->sig2_smem[2] = smC;
+    if ((rc = sigma2_attributes<double>(h))) return rc;
+    if (h->precision == QS_PREC_MIXED && (rc = sigma2_attributes<float>(h))) return rc;
     // every buffer is zeroed on h->stream by dalloc: the tables are copied on the same
     // stream (after the zeroing) and the host staging vectors must outlive the copies
     QS_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
 
-int sigma2_compute(qs_handle *h, const double *d_x) {
+// Y and V hold FP32 spectra when T = float (in the first half of the same allocations)
+template <typename T> static int sigma2_run(qs_handle *h, const double *d_x) {
     const FftPlan &fp = h->fft;
     const int nA = h->nA;
     const bool pers = persistent_AC(fp);
+    cplx<T> *Y = (cplx<T> *)h->d_Y, *V = (cplx<T> *)h->d_V;
     int pa = prof_begin(h, K_SIG2A);
     if (pers) {
         const int nitems = (int)((h->nY + 3) / 4) * (fp.N2 / 4);
-        pick_fwdA_p(fp.N1)<<<std::min(nitems, 148), 512, smem_fwdA_p(fp.N1), h->stream>>>(
-            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, h->d_Y, nitems);
+        pick_fwdA_p<T>(fp.N1)<<<std::min(nitems, 148), 512, smem_fwdA_p<T>(fp.N1), h->stream>>>(
+            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, nitems);
     } else {
         dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
-        pick_fwdA(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, h->sig2_smem[0], h->stream>>>(
-            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, h->d_Y, h->sig2_SA, h->sig2_GA);
+        pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, smem_A<T>(h), h->stream>>>(
+            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, h->sig2_SA, h->sig2_GA);
     }
     prof_end(h, pa);
     QS_CUDA(h, cudaGetLastError());
@@ -743,24 +781,34 @@ int sigma2_compute(qs_handle *h, const double *d_x) {
         const int nitems = h->sig2_npairs * (fp.N1 / 2 + 1);
         const int gB = std::min(nitems, 148);  // persistent: one block per SM
         int pb = prof_begin(h, K_SIG2B);
-        pick_mid(fp.N2)<<<gB, 512, h->sig2_smem[1], h->stream>>>(h->d_Y, h->d_V, h->sig2_pairs, nA, fp, h->d_tw,
-                                                                 nitems);
+        pick_mid<T>(fp.N2)<<<gB, 512, smem_B<T>(h), h->stream>>>(Y, V, h->sig2_pairs, nA, fp, h->d_tw, nitems);
         prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
     int pc = prof_begin(h, K_SIG2C);
     if (pers) {
         const int nitems = 2 * h->nAs * h->nAs * (fp.N2 / 4);
-        pick_invC_p(fp.N1)<<<std::min(nitems, 148), 512, smem_invC_p(fp.N1), h->stream>>>(
-            h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
+        pick_invC_p<T>(fp.N1)<<<std::min(nitems, 148), 512, smem_invC_p<T>(fp.N1), h->stream>>>(
+            V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
     } else {
         dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
-        pick_invC(fp.N1, h->sig2_GC)<<<gC, 256, h->sig2_smem[2], h->stream>>>(
-            h->d_V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
+        pick_invC<T>(fp.N1, h->sig2_GC)<<<gC, 256, smem_C<T>(h), h->stream>>>(
+            V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
     }
     prof_end(h, pc);
     QS_CUDA(h, cudaGetLastError());
     return 0;
+}
+
+int sigma2_compute(qs_handle *h, const double *d_x, bool fp32) {
+    if (fp32) {
+        if (h->precision != QS_PREC_MIXED) {
+            h->err = "sigma2: FP32 transforms need a QS_PREC_MIXED handle";
+            return -1;
+        }
+        return sigma2_run<float>(h, d_x);
+    }
+    return sigma2_run<double>(h, d_x);
 }
 
 }  // namespace qs

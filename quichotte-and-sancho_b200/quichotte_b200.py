@@ -84,7 +84,7 @@ class QsScfResult(ctypes.Structure):
                 ("aborted", ctypes.c_int), ("runaway", ctypes.c_int), ("unphysical", ctypes.c_int),
                 ("i_worst", ctypes.c_int), ("n_worst", ctypes.c_double), ("w_worst", ctypes.c_double),
                 ("n_resets", ctypes.c_int), ("log", ctypes.POINTER(QsScfStep)), ("log_cap", ctypes.c_int),
-                ("n_log", ctypes.c_int), ("seconds", ctypes.c_double)]
+                ("n_log", ctypes.c_int), ("seconds", ctypes.c_double), ("n_mixed", ctypes.c_int)]
 
 
 RESIDUAL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, _dp, _dp, _ip)
@@ -262,7 +262,7 @@ class Solver:
         r.log, r.log_cap = log, cap
         self._check(self._f("solve_scf")(self._h, V, int(fresh_start), ctypes.byref(r)), "solve_scf")
         out = {k: getattr(r, k) for k in ("converged", "n_iter", "fmax", "aborted", "runaway", "unphysical",
-                                           "i_worst", "n_worst", "w_worst", "n_resets", "seconds")}
+                                           "i_worst", "n_worst", "w_worst", "n_resets", "seconds", "n_mixed")}
         out["converged"] = bool(out["converged"])
         out["log"] = [(log[i].step, log[i].fmax, log[i].rms, log[i].nh) for i in range(r.n_log)]
         return out

@@ -189,3 +189,39 @@ def test_fft_lengths_cover_all_radices():
         m = small_helix(d)
         seen |= radices(qb.Solver(m).Nf)
     assert seen == {2, 3, 5, 7}, seen
+
+
+# ---- mixed precision (QS_PREC_MIXED) ----
+
+MIXED_SIGMA_DELTAS = [0.05, 0.0029, 0.0037309, 0.0004655]  # Nf = 315, 5250, 4096, 32768
+
+
+@pytest.mark.parametrize("delta", MIXED_SIGMA_DELTAS)
+def test_mixed_sigma2_within_fp32_tolerance_of_oracle(delta):
+    """FP32 transforms, 2x2 algebra and spectra: Sigma2 within 2e-5 relative of the FP64
+    oracle (FP32 rounding over log2(Nf) FFT passes and the cubic products)."""
+    m = small_helix(delta)
+    gs, os_ = qb.Solver(m, precision=qb.QS_PREC_MIXED), oracle_lib.solver(m)
+    x = os_.initial_vector(0.3)
+    x = x + 1e-3 * np.random.default_rng(4).standard_normal(x.size)
+    SRg, SLg, _ = gs.self_energies(x)
+    SRo, SLo, _ = os_.self_energies(x)
+    assert rel(SRg, SRo) < 2e-5 and rel(SLg, SLo) < 2e-5, (rel(SRg, SRo), rel(SLg, SLo))
+    assert rel(SRg, SRo) > 1e-12  # the FP32 path ran
+
+
+@pytest.mark.parametrize("case", ORDER2)
+def test_mixed_solve_matches_fp64_solve(case):
+    """A mixed solve converges on FP64 residuals: currents, occupations and the spectral
+    function agree with the plain FP64 solve to far better than 1e-6 relative."""
+    m = qb.Model.load(os.path.join(CASES, case))
+    f64, mix = qb.Solver(m), qb.Solver(m, precision=qb.QS_PREC_MIXED)
+    r64, rmx = f64.solve_scf(m.V), mix.solve_scf(m.V)
+    assert r64["converged"] and rmx["converged"]
+    assert rmx["n_mixed"] > 0 and r64["n_mixed"] == 0
+    j64, jmx = np.array(f64.current(m.V)), np.array(mix.current(m.V))
+    assert np.max(np.abs(jmx - j64)) <= 1e-6 * np.max(np.abs(j64)), (j64, jmx)
+    o64, omx = f64.observables(), mix.observables()
+    for k in o64:
+        a, b_ = np.asarray(omx[k]), np.asarray(o64[k])
+        assert np.max(np.abs(a - b_)) <= 1e-6 * max(np.max(np.abs(b_)), 1e-300), k
