@@ -143,6 +143,50 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
 enum { QS_ERR_NOALLOC_LIMIT = -1001 };
 int qs_invert_batched_noalloc(int N, int batch, double *A, int *info, void *stream);
 
+/* ---- memory (setup_storage's memory estimate, src/green_functions.f90:90-190) ---- */
+
+/* Device memory (GiB) a solve of this problem keeps from qs_create to qs_destroy: the
+ * allocations of qs_create, computed on the host without a device. */
+int qs_estimate_bytes(const qs_problem *p, double *gib);
+/* Device memory (GiB) the handle has allocated. */
+double qs_device_bytes(const qs_handle *h);
+
+/* ---- serving (no counterpart in the reference, whose program solves the voltages of one
+ * model one after another, src/quichotte.f90:125-143) ----
+ * A request is one IV point: a problem (model + energy grid, arrays copied at submit) and
+ * a voltage, solved from a fresh start as qs_create + qs_solve_scf + qs_current. Requests
+ * are admitted in arrival order as soon as a worker is free and the estimated device
+ * memory of the solve fits into the budget left by the solves in flight; admitted solves
+ * keep their state on the device and run concurrently on their own streams and threads
+ * (continuous batching). A request that exceeds the whole budget is refused at submit
+ * (QS_ERR_TOO_LARGE). Times are seconds on the server's clock (qs_server_clock). */
+enum { QS_ERR_TOO_LARGE = -1002 };
+typedef struct qs_server qs_server;
+typedef struct qs_server_config {
+    int device;
+    int max_inflight;      /* solves on the device at once, 1..64                    */
+    double hbm_budget_gib; /* admission budget; <= 0: 90% of the free HBM at creation */
+} qs_server_config;
+typedef struct qs_request_result {
+    int64_t id;
+    int status;            /* 0, or the qs_create / qs_solve_scf status               */
+    int converged, n_iter, n_mixed;
+    double fmax, J_up, J_down;
+    double solve_s;        /* device time of the solve                                */
+    double t_arrival, t_start, t_done; /* submit, admission, completion              */
+    double device_gib;     /* admitted memory (estimate + headroom)                  */
+    char error[160];       /* qs_last_error of a failed request, else empty           */
+} qs_request_result;
+int qs_server_create(const qs_server_config *cfg, qs_server **s);
+int qs_server_submit(qs_server *s, const qs_problem *p, double V, int64_t id);
+/* Copies up to cap finished results into out, waiting up to timeout_s for the first. */
+int qs_server_poll(qs_server *s, qs_request_result *out, int cap, double timeout_s);
+int qs_server_pending(qs_server *s); /* submitted and not yet returned by poll */
+double qs_server_clock(const qs_server *s);
+double qs_server_budget_gib(const qs_server *s);
+/* Waits for the solves in flight; queued requests that were never admitted are dropped. */
+void qs_server_destroy(qs_server *s);
+
 /* ---- instrumentation (no counterpart in the reference, whose only timer is the
  * wall clock of src/quichotte.f90:50-58) ---- */
 

@@ -207,6 +207,16 @@ namespace qs {
     } while (0)
 
 int dalloc(qs_handle *h, void **p, size_t bytes);
+// The dynamic shared-memory cap of a kernel is a process-wide attribute: it is always set
+// to the device maximum (a cap, not a reservation), so that handles that size the same
+// kernel differently, on other threads, never lower it under each other's launches.
+inline cudaError_t smem_cap(const void *kernel) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(SMEM_MAX - fa.sharedSizeBytes));
+}
 
 // every kernel launch of the library is counted (qs_kernel_launches)
 void count_launch();

@@ -50,9 +50,11 @@ void prof_end(qs_handle *h, int idx) {
 int dalloc(qs_handle *h, void **p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    // stream-ordered: releasing a handle's memory does not synchronise the device, so
+    // solves of other handles (the serving loop) keep running meanwhile
+    cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
     if (e != cudaSuccess) {
-        h->err = "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
+        h->err = "cudaMallocAsync of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
         *p = nullptr;
         return -2;
     }
@@ -64,6 +66,12 @@ int dalloc(qs_handle *h, void **p, size_t bytes) {
     h->allocs.push_back(*p);
     h->bytes_allocated += bytes;
     return 0;
+}
+
+void release_all(qs_handle *h) {
+    for (void *p : h->allocs) cudaFreeAsync(p, h->stream);
+    h->allocs.clear();
+    cudaStreamSynchronize(h->stream);
 }
 
 // G^<(t=0) on the on-site blocks of the active sites from the SCF vector, then Sigma1
@@ -479,13 +487,8 @@ template <class T> int upload(qs_handle *h, T **d, const std::vector<T> &v) {
 
 // ------------------------------------------------------------------------------------
 // C ABI
-// ------------------------------------------------------------------------------------
-extern "C" {
-
-int qs_create(const qs_problem *p, qs_handle **out) {
-    *out = nullptr;
-    auto *h = new qs_handle();
-    *out = h;
+// the host fields of a handle from the problem (no device work)
+static int fill_host(qs_handle *h, const qs_problem *p) {
     h->Norb = p->Norb;
     h->N_sites = p->N_sites;
     h->N_atoms = p->N_atoms;
@@ -504,6 +507,10 @@ int qs_create(const qs_problem *p, qs_handle **out) {
     h->maxscf = p->maxscf;
     h->single = p->single_history != 0;
     const int N = h->Norb;
+    if (N > 512 || N < 2 || h->n < 1) {
+        h->err = "qs_create: need 2 <= Norb <= 512 and n_omega >= 1";
+        return -1;
+    }
     const size_t nn = (size_t)N * N;
     h->H.assign(p->H, p->H + 2 * nn);
     h->GammaL.assign(p->GammaL, p->GammaL + 2 * nn);
@@ -512,10 +519,6 @@ int qs_create(const qs_problem *p, qs_handle **out) {
     h->omega.assign(p->omega, p->omega + h->n);
     h->atom_norb.assign(p->atom_norb, p->atom_norb + p->N_atoms);
     h->atom_first.assign(p->atom_first, p->atom_first + p->N_atoms);
-    if (N > 512 || N < 2 || h->n < 1) {
-        h->err = "qs_create: need 2 <= Norb <= 512 and n_omega >= 1";
-        return -1;
-    }
     if (h->precision != QS_PREC_FP64 && h->precision != QS_PREC_MIXED) {
         h->err = "qs_create: precision must be QS_PREC_FP64 or QS_PREC_MIXED";
         return -1;
@@ -524,6 +527,52 @@ int qs_create(const qs_problem *p, qs_handle **out) {
         h->err = "qs_create: nhist must be in 0..32";
         return -1;
     }
+    return 0;
+}
+
+// device bytes a solve keeps (the allocations of qs_create), after setup_storage
+static size_t handle_need(const qs_handle *h) {
+    const int N = h->Norb, nA = h->nA, n = h->n;
+    const size_t nn = (size_t)N * N, zc_ = sizeof(zc);
+    const size_t hist_el = h->single ? 4 : 8;
+    const int Nf = (h->order == 2) ? good_fft_size_h(2 * n - 1) : 0;
+    size_t need = 0;
+    need += nn * zc_ * 2 + (size_t)n * 8 * 1;                                // Hemb, Sig1, omega
+    need += (size_t)n * (4 * h->N_sites * zc_ + N * 8 + 16);                // onsL, dosd, trU, trD
+    if (h->has_atomL) need += (size_t)n * h->atom_off.back() * zc_;
+    need += (size_t)n * std::max(nA, 1) * zc_ * 2;                           // gRd, gLd
+    if (!dyson_fits_smem(N)) need += (size_t)148 * 2 * nn * zc_;            // Gauss-Jordan workspace
+    if (h->order == 2) {
+        size_t nY = (size_t)nA * nA + (size_t)nA * (nA + 1) / 2;
+        need += (size_t)h->n_vec * 8 * 4;                                     // x, F, Fold, xold
+        need += (size_t)h->n_vec * hist_el * 2 * h->nhist;                    // history
+        need += (size_t)n * nA * nA * zc_ * 2;                                // SigR, SigL
+        need += (nY + (size_t)2 * nA * nA) * Nf * zc_;                        // Y, V
+    } else {
+        const size_t G_chunk = std::max<size_t>(1, std::min<size_t>((size_t)n, (2ull << 30) / (nn * zc_)));
+        need += G_chunk * nn * zc_;                                           // full-G chunk
+        need += (size_t)148 * 4 * N * std::max(h->nS, 1) * zc_;               // sweep scratch
+        const int64_t nv = std::max<int64_t>(h->n_vec, 1);
+        if (h->order == 1) need += (size_t)nv * 8 * 4 + (size_t)nv * hist_el * 2 * h->nhist;
+    }
+    need += broyden_red_len() * 8 + (size_t)3 * h->nS * h->nS * zc_;        // reductions, Gamma blocks
+    if (h->order == 2) {
+        size_t nY = (size_t)nA * nA + (size_t)nA * (nA + 1) / 2;
+        need += (size_t)Nf * zc_ + nY * 8 + (size_t)h->nAs * h->nAs * 16;      // twiddles, FFT tables
+    }
+    need += (size_t)1 << 20;  // index tables and the allocations' 256-byte granularity
+    return need;
+}
+
+// ------------------------------------------------------------------------------------
+extern "C" {
+
+int qs_create(const qs_problem *p, qs_handle **out) {
+    *out = nullptr;
+    auto *h = new qs_handle();
+    *out = h;
+    int rc0 = fill_host(h, p);
+    if (rc0) return rc0;
     QS_CUDA(h, cudaSetDevice(h->device));
     QS_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     QS_CUDA(h, cudaEventCreate(&h->ev0));
@@ -533,24 +582,14 @@ int qs_create(const qs_problem *p, qs_handle **out) {
         h->err = "qs_create: more than 32 left-contact states";
         return -1;
     }
+    const int N = h->Norb;
+    const size_t nn = (size_t)N * N;
     const int nA = h->nA, nS = h->nS, n = h->n;
     const int Nf = (h->order == 2) ? good_fft_size_h(2 * n - 1) : 0;
-
-    // ---- HBM admission: everything this solve keeps on the device
     const size_t zc_ = sizeof(zc);
     size_t hist_el = h->single ? 4 : 8;
-    size_t need = 0;
-    need += nn * zc_ * 2 + (size_t)n * 8 * 1;                                // Hemb, Sig1, omega
-    need += (size_t)n * (4 * h->N_sites * zc_ + N * 8 + 16);                // onsL, dosd, trU, trD
-    if (h->has_atomL) need += (size_t)n * h->atom_off.back() * zc_;
-    if (h->order >= 1) need += (size_t)n * nA * zc_ * 2;                     // gRd, gLd
-    if (h->order == 2) {
-        size_t nY = (size_t)nA * nA + (size_t)nA * (nA + 1) / 2;
-        need += (size_t)h->n_vec * 8 * 4;                                     // x, F, Fold, xold
-        need += (size_t)h->n_vec * hist_el * 2 * h->nhist;                    // history
-        need += (size_t)n * nA * nA * zc_ * 2;                                // SigR, SigL
-        need += (nY + (size_t)2 * nA * nA) * Nf * zc_;                        // Y, V
-    }
+    // ---- HBM admission: everything this solve keeps on the device
+    size_t need = handle_need(h);
     size_t freeb = 0, totb = 0;
     QS_CUDA(h, cudaMemGetInfo(&freeb, &totb));
     if (need + (512ull << 20) > freeb) {
@@ -645,7 +684,7 @@ void qs_destroy(qs_handle *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
-    for (void *p : h->allocs) cudaFree(p);
+    release_all(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -653,6 +692,17 @@ void qs_destroy(qs_handle *h) {
 }
 
 const char *qs_last_error(const qs_handle *h) { return h ? h->err.c_str() : "no handle"; }
+
+int qs_estimate_bytes(const qs_problem *p, double *gib) {
+    qs_handle h;
+    int rc = fill_host(&h, p);
+    if (rc) return rc;
+    setup_storage(&h);
+    *gib = (double)handle_need(&h) / (double)(1ull << 30);
+    return 0;
+}
+
+double qs_device_bytes(const qs_handle *h) { return h ? (double)h->bytes_allocated / (double)(1ull << 30) : 0.0; }
 
 int64_t qs_kernel_launches(void) { return g_launches.load(); }
 
@@ -1031,8 +1081,7 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
             for (int i = 0; i < (int)bo.log.size() && i < log_cap; i++) log[i] = bo.log[i];
         }
     }
-    cudaStreamSynchronize(h.stream);
-    for (void *p : h.allocs) cudaFree(p);
+    release_all(&h);
     cudaStreamDestroy(h.stream);
     return rc;
 }

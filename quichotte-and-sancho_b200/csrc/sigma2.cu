@@ -652,17 +652,12 @@ static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p<double>(fp.N1)
 
 template <typename T> static int sigma2_attributes(qs_handle *h) {
     const FftPlan &fp = h->fft;
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA),
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_A<T>(h)));
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_mid<T>(fp.N2), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_B<T>(h)));
-    QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC<T>(fp.N1, h->sig2_GC),
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_C<T>(h)));
+    QS_CUDA(h, smem_cap((const void *)pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA)));
+    QS_CUDA(h, smem_cap((const void *)pick_mid<T>(fp.N2)));
+    QS_CUDA(h, smem_cap((const void *)pick_invC<T>(fp.N1, h->sig2_GC)));
     if (persistent_AC(fp)) {
-        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_fwdA_p<T>(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_fwdA_p<T>(fp.N1)));
-        QS_CUDA(h, cudaFuncSetAttribute((const void *)pick_invC_p<T>(fp.N1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_invC_p<T>(fp.N1)));
+        QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1)));
+        QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1)));
     }
     return 0;
 }

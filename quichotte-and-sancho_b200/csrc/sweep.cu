@@ -1000,7 +1000,7 @@ static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
     const int N = a.N;
     if (use_blocked(N)) {
         size_t sm = (size_t)swz_units(N) * sizeof(zc);
-        QS_CUDA(h, cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        QS_CUDA(h, smem_cap((const void *)dyson_bgj));
         a.ws = nullptr;
         int pi = prof_begin(h, K_DYSON);
         dyson_bgj<<<nblocks, BGJ_THREADS, sm, h->stream>>>(a);
@@ -1012,7 +1012,7 @@ static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
     size_t sm = 0;
     if (dyson_fits(N)) {
         sm = dyson_smem(N);
-        QS_CUDA(h, cudaFuncSetAttribute(dyson_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        QS_CUDA(h, smem_cap((const void *)dyson_gj));
         a.ws = nullptr;
     } else {
         nblocks = std::min<int>(nblocks, (int)h->ws_slots);
@@ -1040,7 +1040,7 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
     size_t sm = 0;
     if (use_blocked(N)) {
         sm = (size_t)swz_units(N) * sizeof(zc);
-        cudaError_t e = cudaFuncSetAttribute(dyson_bgj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = smem_cap((const void *)dyson_bgj);
         if (e != cudaSuccess) return -(int)e;
         count_launch();
         dyson_bgj<<<nb, BGJ_THREADS, sm, st>>>(a);
@@ -1049,7 +1049,7 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
     }
     if (dyson_fits(N)) {
         sm = dyson_smem(N);
-        cudaError_t e = cudaFuncSetAttribute(dyson_gj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = smem_cap((const void *)dyson_gj);
         if (e != cudaSuccess) return -(int)e;
     } else {
         a.ws = d_ws;
@@ -1128,7 +1128,7 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         int pi;
         const int nbt = std::min(n, 148);
         if (nA >= 48 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt)) {
-            QS_CUDA(h, cudaFuncSetAttribute(keldysh_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KD_SMEM));
+            QS_CUDA(h, smem_cap((const void *)keldysh_tc));
             pi = prof_begin(h, K_KELDYSH);
             keldysh_tc<<<nbt, 256, KD_SMEM, h->stream>>>(k);
         } else {

@@ -26,6 +26,7 @@ libqsb200.so raises ImportError, there is no CPU fallback.
 import ctypes
 import os
 import subprocess
+import time
 
 import numpy as np
 
@@ -141,8 +142,36 @@ def kernel_launches():
 C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current", "qs_get_observables",
          "qs_vector_length", "qs_active_states", "qs_fft_length", "qs_initial_vector", "qs_residual",
          "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
-         "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc")
+         "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
+         "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
+         "qs_server_budget_gib", "qs_server_destroy")
 QS_ERR_NOALLOC_LIMIT = -1001
+QS_ERR_TOO_LARGE = -1002
+
+
+class QsServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_inflight", ctypes.c_int), ("hbm_budget_gib", ctypes.c_double)]
+
+
+class QsRequestResult(ctypes.Structure):
+    _fields_ = ([("id", ctypes.c_int64)] + [(k, ctypes.c_int) for k in ("status", "converged", "n_iter", "n_mixed")]
+                + [(k, ctypes.c_double) for k in ("fmax", "J_up", "J_down", "solve_s", "t_arrival", "t_start",
+                                                  "t_done", "device_gib")] + [("error", ctypes.c_char * 160)])
+
+
+_lib.qs_estimate_bytes.argtypes = [ctypes.POINTER(QsProblem), _dp]
+_lib.qs_device_bytes.argtypes = [ctypes.c_void_p]
+_lib.qs_device_bytes.restype = ctypes.c_double
+_lib.qs_server_create.argtypes = [ctypes.POINTER(QsServerConfig), ctypes.POINTER(ctypes.c_void_p)]
+_lib.qs_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(QsProblem), ctypes.c_double, ctypes.c_int64]
+_lib.qs_server_poll.argtypes = [ctypes.c_void_p, ctypes.POINTER(QsRequestResult), ctypes.c_int, ctypes.c_double]
+_lib.qs_server_pending.argtypes = [ctypes.c_void_p]
+_lib.qs_server_clock.argtypes = [ctypes.c_void_p]
+_lib.qs_server_clock.restype = ctypes.c_double
+_lib.qs_server_budget_gib.argtypes = [ctypes.c_void_p]
+_lib.qs_server_budget_gib.restype = ctypes.c_double
+_lib.qs_server_destroy.argtypes = [ctypes.c_void_p]
+_lib.qs_server_destroy.restype = None
 _lib.qs_invert_batched_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p]
 
@@ -255,6 +284,10 @@ class Solver:
     def __del__(self):
         self.close()
 
+    def device_gib(self):
+        """Device memory (GiB) this handle has allocated."""
+        return self._f("device_bytes")(self._h)
+
     def solve_scf(self, V, fresh_start=True):
         cap = self.model.maxscf + 2
         log = (QsScfStep * cap)()
@@ -310,6 +343,70 @@ class Solver:
         S1 = np.zeros((m.Norb, m.Norb), np.complex128, order="F")
         self._check(self._f("self_energies")(self._h, _ptr(x), _ptr(SR), _ptr(SL), _ptr(S1)), "self_energies")
         return SR, SL, S1
+
+
+def estimate_gib(model, precision=QS_PREC_FP64, **settings):
+    """Device memory (GiB) a solve of this model keeps (qs_estimate_bytes)."""
+    prob = model.problem(precision, 0, **settings)
+    g = ctypes.c_double()
+    rc = _lib.qs_estimate_bytes(ctypes.byref(prob), ctypes.byref(g))
+    if rc != 0:
+        raise SolverError(f"estimate failed ({rc})")
+    return g.value
+
+
+class Server:
+    """The serving loop (qs_server_*): IV-point requests admitted by HBM budget and solved
+    concurrently on the device (continuous batching)."""
+
+    def __init__(self, device=0, max_inflight=4, hbm_budget_gib=0.0):
+        cfg = QsServerConfig(device, max_inflight, hbm_budget_gib)
+        self._s = ctypes.c_void_p()
+        rc = _lib.qs_server_create(ctypes.byref(cfg), ctypes.byref(self._s))
+        if rc != 0:
+            raise SolverError(f"qs_server_create failed ({rc})")
+
+    @property
+    def budget_gib(self):
+        return _lib.qs_server_budget_gib(self._s)
+
+    def clock(self):
+        return _lib.qs_server_clock(self._s)
+
+    def submit(self, model, V, rid, precision=QS_PREC_FP64, **settings):
+        """Queue one IV point; the problem arrays are copied before this returns.
+        Returns 0 or QS_ERR_TOO_LARGE (never fits the budget)."""
+        prob = model.problem(precision, 0, **settings)
+        rc = _lib.qs_server_submit(self._s, ctypes.byref(prob), V, rid)
+        if rc not in (0, QS_ERR_TOO_LARGE):
+            raise SolverError(f"qs_server_submit failed ({rc})")
+        return rc
+
+    def pending(self):
+        return _lib.qs_server_pending(self._s)
+
+    def poll(self, timeout=0.0, cap=64):
+        buf = (QsRequestResult * cap)()
+        k = _lib.qs_server_poll(self._s, buf, cap, timeout)
+        out = [{f: getattr(buf[i], f) for f, _ in QsRequestResult._fields_} for i in range(k)]
+        for r in out:
+            r["error"] = r["error"].decode(errors="replace")
+        return out
+
+    def drain(self, timeout=3600.0):
+        """Results of every request still pending."""
+        out, t0 = [], time.time()
+        while self.pending() > 0 and time.time() - t0 < timeout:
+            out += self.poll(timeout=1.0)
+        return out
+
+    def close(self):
+        if getattr(self, "_s", None):
+            _lib.qs_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        self.close()
 
 
 def invert_batched(A, precision=QS_PREC_FP64, lib=None, prefix="qs_"):
