@@ -9,7 +9,12 @@ continuation from the previous one, then Current and the observables):
   steps of 0.05 V (41 voltages), Broyden: reference defaults (alpha_mix 0.5, 16-column
   single-precision history, tolf 1e-6). Synthetic input (the model is analytic).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--precision both|fp64|mixed]
+                  [--serve R] [--serve-rate r] [--serve-inflight k]
+
+Default: the FP64 form, then the mixed form (the headline value), their ratio and the
+current error of the mixed form against the FP64 one; then a serving stream (p50/p99
+latency of IV-point requests through qs_server).
 
 N > 1 (launched with torch.distributed.run): replicas. Rank r solves its own contiguous
 block of the voltage sweep; no data-path collective. value = all IV points / max over
@@ -137,6 +142,57 @@ def cpu_baseline_sample(n_sample=4096, steps_per_point=STEPS_PER_POINT, threads=
                       f"x{steps_per_point:g} SCF steps per IV point; Broyden update not counted"}
 
 
+def serving_requests(qb, n_req, seed=2024):
+    """The serving stream: seeded random helices (sites/turn in [3,12], turns in [1,8],
+    U ~ U[0.2,1.5] eV, V ~ U[-1,1] V, n_omega in {4096, 8192, 16384, 32768} on [-10,10] eV,
+    t = 1 eV, lambda = 0.01 eV, Gamma = 0.5 eV, T = 300 K, 2nd order)."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n_req):
+        ions, turns = int(rng.integers(3, 13)), int(rng.integers(1, 9))
+        U, V = float(rng.uniform(0.2, 1.5)), float(rng.uniform(-1.0, 1.0))
+        n = int(rng.choice([4096, 8192, 16384, 32768]))
+        args = dict(N_ions=ions, N_turns=turns, hel_length=PITCH * turns * (ions - 1) / ions, hel_radius=RADIUS,
+                    hand=1.0, E_CC=0.0, t_hop=1.0, lamb=0.01, U_int=U, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5,
+                    T=300.0, mu=0.0, order=2)
+        ev = np.linalg.eigvalsh(qb.Model.helix(dw=1.0, up=1.0, delta=0.1, **args).H)
+        delta = 20.0 / n
+        m = qb.Model.helix(dw=ev[0] + 10.0, up=10.0 - ev[-1] + 0.5 * delta, delta=delta, **args)
+        reqs.append((k, m, V, 2 * ions * turns))
+    return reqs
+
+
+def run_serving(qb, n_req, rate, max_inflight, precision):
+    """Requests submitted at Poisson arrival times (rate per second) to a qs_server; returns
+    latency percentiles (arrival to completion) and throughput."""
+    reqs = serving_requests(qb, n_req)
+    settings = dict(alpha_mix=0.5, nhist=8, tolf=1e-6, maxscf=300, single_history=1)
+    srv = qb.Server(max_inflight=max_inflight)
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    refused, results = [], []
+    t0 = time.perf_counter()
+    t_next = 0.0
+    for (k, m, V, norb), gap in zip(reqs, gaps):
+        t_next += gap
+        while time.perf_counter() - t0 < t_next:
+            results += srv.poll(timeout=min(0.05, max(0.0, t_next - (time.perf_counter() - t0))))
+        if srv.submit(m, V, k, precision=precision, **settings) != 0:
+            refused.append(k)
+    results += srv.drain()
+    srv.close()
+    ok = [r for r in results if r["status"] == 0]
+    lat = np.array([r["t_done"] - r["t_arrival"] for r in ok])
+    span = max(r["t_done"] for r in ok) - min(r["t_arrival"] for r in ok) if ok else 0.0
+    conv = sum(int(r["converged"]) for r in ok)
+    return {"requests": n_req, "arrival_rate_per_s": rate, "max_inflight": max_inflight, "served": len(ok),
+            "converged": conv, "refused_too_large": len(refused), "failed": len(results) - len(ok),
+            "p50_s": float(np.percentile(lat, 50)) if ok else None, "p99_s": float(np.percentile(lat, 99)) if ok else None,
+            "mean_solve_s": float(np.mean([r["solve_s"] for r in ok])) if ok else None,
+            "throughput_per_s": conv / span if span > 0 else 0.0, "span_s": span,
+            "orbitals": [int(x[3]) for x in reqs]}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the oracle (a restatement of the reference's CPU path: OpenMP
     over energies, LAPACK zgetrf/zgetri from OpenBLAS, its own FFT) on the host cores."""
@@ -174,6 +230,10 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
     ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
+    ap.add_argument("--serve", type=int, default=16,
+                    help="requests of the serving stream (0: none; the full stream is 512)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-inflight", type=int, default=4, help="solves on the device at once")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="both: the FP64 form, then the mixed form (headline value), with their ratio")
     args = ap.parse_args()
@@ -316,6 +376,12 @@ def main():
             line["mixed_over_fp64"] = head["value"] / f64["value"] if f64["value"] > 0 else None
             line["current_rel_err_vs_fp64"] = float(np.max(np.abs(jmx - j64)) / np.max(np.abs(j64)))
             line["kernel_ms_mixed"] = {k: round(v[0], 3) for k, v in head["prof"].items() if v[1]}
+        if world == 1 and args.serve > 0:
+            line["serving"] = run_serving(qb, args.serve, args.serve_rate, args.serve_inflight, qb.QS_PREC_FP64)
+            line["serving"]["workload"] = (f"serving stream, first {args.serve} of the seeded 512-request stream: random "
+                                           "helices, sites/turn 3-12, turns 1-8, U 0.2-1.5 eV, V -1..1 V, 4096-32768 "
+                                           "energies, Poisson arrivals; one fresh-start IV point per request, FP64, "
+                                           "Broyden nhist 8; requests above the HBM budget are refused")
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.ref_sample)
         print(json.dumps(line), flush=True)
