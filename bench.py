@@ -142,6 +142,24 @@ def cpu_baseline_sample(n_sample=4096, steps_per_point=STEPS_PER_POINT, threads=
                       f"x{steps_per_point:g} SCF steps per IV point; Broyden update not counted"}
 
 
+def voltage_block(rank, world, volts=VOLTS):
+    """Replica r's contiguous block of the voltage sweep (no data-path collective: each
+    replica continues along its own block)."""
+    per = (len(volts) + world - 1) // world
+    return volts[rank * per:(rank + 1) * per] or volts[-1:]
+
+
+def reduce_replicas(dev_s, wall, n_conv, device="cpu"):
+    """Max over ranks of the device and wall times, sum of the converged points."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([dev_s, wall], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(n_conv)], device=device, dtype=torch.float64)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), int(c[0])
+
+
 def serving_requests(qb, n_req, seed=2024):
     """The serving stream: seeded random helices (sites/turn in [3,12], turns in [1,8],
     U ~ U[0.2,1.5] eV, V ~ U[-1,1] V, n_omega in {4096, 8192, 16384, 32768} on [-10,10] eV,
@@ -254,9 +272,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
 
     m = model_cfg1(qb, args.n_omega)
-    # this rank's block of the voltage sweep
-    per = (len(VOLTS) + world - 1) // world
-    block = VOLTS[rank * per:(rank + 1) * per] or VOLTS[-1:]
+    block = voltage_block(rank, world)
     seq = [block[k % len(block)] for k in range(args.warmup + args.steps)]
     fresh = [k == 0 or (k % len(block) == 0) for k in range(len(seq))]
     obs_bytes = 8 * (2 * m.Norb * m.Norb + m.Norb * m.n_omega + 2 * m.n_omega)
@@ -297,11 +313,7 @@ def main():
                    mixed_steps=mixed_steps, currents=currents, nA=solver.nA, Nf=solver.Nf, n_vec=solver.n_vec)
         solver.close()
         if world > 1:
-            t = torch.tensor([dev_s, wall, float(n_conv)], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
-            tc = t[2:].clone()
-            dist.all_reduce(tc, op=dist.ReduceOp.SUM)
-            dev_s, wall, n_conv = float(t[0]), float(t[1]), int(tc[0])
+            dev_s, wall, n_conv = reduce_replicas(dev_s, wall, n_conv, device="cuda")
             dist.barrier()
         out.update(dev_s=dev_s, wall=wall, n_conv=n_conv, value=n_conv / dev_s if dev_s > 0 else 0.0,
                    e2e=n_conv / wall if wall > 0 else 0.0)
