@@ -299,13 +299,20 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                         const double id = 1.0 / fma(R[0].x, R[0].x, R[0].y * R[0].y);
                         inv_own = zc{R[0].x * id, -R[0].y * id};
                     }
-                    // pivot search: the warp maximum of cabs1, then its lowest lane (first maximum)
-                    const double v = valid ? cabs1(R[0]) : -1.0;
-                    double m = v;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-                    const unsigned bal = __ballot_sync(0xffffffffu, valid && v == m);
+                    // pivot search: the warp maximum of cabs1, then its lowest lane (first
+                    // maximum). cabs1 >= 0, so its bit pattern orders like its value: two
+                    // integer warp reductions (high word + 1, 0 for rows not searched; then the
+                    // low word among the lanes holding the maximal high word) replace a chain
+                    // of FP64 shuffles
+                    const double v = valid ? cabs1(R[0]) : 0.0;
+                    const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
+                    const unsigned hk = valid ? (unsigned)(bits >> 32) + 1u : 0u, lk = (unsigned)bits;
+                    const unsigned mh = __reduce_max_sync(0xffffffffu, hk);
+                    const unsigned ml = __reduce_max_sync(0xffffffffu, hk == mh ? lk : 0u);
+                    const unsigned bal = __ballot_sync(0xffffffffu, valid && hk == mh && lk == ml);
                     const int wl = bal ? __ffs(bal) - 1 : 32;
+                    const double m =
+                        mh ? __longlong_as_double((long long)(((unsigned long long)(mh - 1u) << 32) | ml)) : -1.0;
                     if (lane == 0) {
                         cand_v[warp] = m;
                         cand_i[warp] = bal ? 32 * warp + wl : N;
