@@ -421,21 +421,23 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int nst = (nY + SA - 1) / SA;
     const int m1max = (n + N2 - 1) / N2;  // zero padding beyond n energies
-    zc *stg0 = (zc *)smem_raw;                                          // 2 x NS staging sequences
-    cplx<T> *wb = F64 ? nullptr : (cplx<T> *)(stg0 + 2 * NS * PL);     // FP32 work sequences
-    cplx<T> *twL = F64 ? (cplx<T> *)(stg0 + 2 * NS * PL) : wb + NS * PL;  // W_N1^m, m < N1
-    cplx<T> *twc = twL + N1;  // W_Nf^{m2 l1} of the tile's four columns, [l1][m2 - m20]
+    zc *stg0 = (zc *)smem_raw;      // 2 x NS staging sequences
+    zc *twc0 = stg0 + 2 * NS * PL;  // 2 x W_Nf^{m2 l1} of a tile's four columns, [l1][m2 - m20]
+    cplx<T> *wb = F64 ? nullptr : (cplx<T> *)(twc0 + 2 * GA * N1);          // FP32 work sequences
+    cplx<T> *twL = F64 ? (cplx<T> *)(twc0 + 2 * GA * N1) : wb + NS * PL;    // W_N1^m, m < N1
     for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
-    auto load = [&](int it, zc *b) {
+    // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores);
+    // blockDim.x is a multiple of 16, so a thread keeps its (sequence, m2) on every tile
+    const int gl_t = threadIdx.x & 3, sl_t = (threadIdx.x >> 2) & 3;
+    auto load = [&](int it, zc *b, zc *twc) {
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
-        // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores)
+        const int s = s0 + sl_t, m2 = m20 + gl_t;
+        const int2 d = s < nY ? desc[s] : int2{-1, 0};
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int gl = t & 3, r = t >> 2, sl = r & 3, m1 = r >> 2;
-            const int s = s0 + sl, m2 = m20 + gl;
+            const int m1 = t >> 4;
             const int64_t w = (int64_t)N2 * m1 + m2;
-            zc *dst = b + (sl * GA + gl) * PL + pidx(m1);
+            zc *dst = b + (sl_t * GA + gl_t) * PL + pidx(m1);
             if (m1 < m1max && s < nY && w < n) {
-                const int2 d = desc[s];
                 const double *blk = X + w * nblk;
                 if (d.x >= 0 && d.y == d.x + 1 && ((reinterpret_cast<uintptr_t>(blk + d.x) & 15) == 0)) {
                     cp_async16(dst, blk + d.x);
@@ -448,20 +450,21 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
                 *dst = zc{0.0, 0.0};
             }
         }
+        for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
+            const int g2 = t & 3, l1 = t >> 2;
+            cp_async16(&twc[t], &tw[(size_t)(m20 + g2) * l1]);
+        }
     };
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
-    if (blockIdx.x < nitems) load(blockIdx.x, stg0);
+    if (blockIdx.x < nitems) load(blockIdx.x, stg0, twc0);
     cp_async_commit();
     int cur = 0;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int nxt = it + gridDim.x;
-        if (nxt < nitems) load(nxt, stg0 + (cur ^ 1) * NS * PL);
+        if (nxt < nitems) load(nxt, stg0 + (cur ^ 1) * NS * PL, twc0 + (cur ^ 1) * GA * N1);
         cp_async_commit();
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
-        for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
-            const int gl = t & 3, l1 = t >> 2;
-            twc[t] = cvt<T>(tw[(size_t)(m20 + gl) * l1]);
-        }
+        const zc *twc = twc0 + cur * GA * N1;
         cp_async_wait1();
         __syncthreads();
         cplx<T> *b;
@@ -479,9 +482,9 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
             const int gl = t & 3, sl = (t >> 2) & 3, l1 = t >> 4;
             const int s = s0 + sl, m2 = m20 + gl;
-            if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * twc[l1 * GA + gl];
+            if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * cvt<T>(twc[l1 * GA + gl]);
         }
-        __syncthreads();  // the buffers and twc are rewritten by the next tiles
+        __syncthreads();  // the buffers are rewritten by the next tiles
         cur ^= 1;
     }
 }
@@ -633,7 +636,8 @@ template <typename T> static InvCPFn<T> pick_invC_p(int N1) {
 }
 template <typename T> static size_t smem_fwdA_p(int N1) {
     const size_t PL = padded_len(N1);
-    return sizeof(zc) * 2 * 16 * PL + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * 16 * PL) + sizeof(cplx<T>) * 5 * N1;
+    return sizeof(zc) * (2 * 16 * PL + 2 * 4 * (size_t)N1) + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * 16 * PL) +
+           sizeof(cplx<T>) * N1;
 }
 template <typename T> static size_t smem_invC_p(int N1) {
     return sizeof(cplx<T>) * ((size_t)2 * 16 * padded_len(N1) + (size_t)N1);
