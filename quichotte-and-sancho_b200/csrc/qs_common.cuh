@@ -15,6 +15,7 @@
 //   gRd, gLd           diagonals (n x nA complex) for the sanity check.
 //   onsL, dosd, atomL, trU, trD   final-sweep arrays, energy-major (reference layout).
 #pragma once
+#include <functional>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -228,6 +229,16 @@ void prof_end(qs_handle *h, int idx);
 int sigma2_setup(qs_handle *h);
 // fp32: FFTs, 2x2 algebra and spectra in FP32 (QS_PREC_MIXED handles), Sigma written in FP64
 int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
+// autotuner (autotune.cu): kinds of decisions and the variants they choose between
+enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1 };
+enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2 };
+int tune_get(int kind, int size);
+bool tune_enabled();
+void tune_put(int kind, int size, int choice);
+// launch(cand[c]) for the recorded choice of (kind, size); the first time, every candidate
+// is launched and timed and the fastest recorded. fallback: the choice without tuning.
+int tune_launch(qs_handle *h, int kind, int size, const int *cand, int ncand, int fallback,
+                const std::function<int(int)> &launch);
 // max |v_i| over a device vector (uses the Broyden reduction scratch)
 int vec_maxabs(qs_handle *h, const double *d_v, int64_t n, double &mx);
 int equal_time_lesser_sigma1(qs_handle *h, const double *d_x);

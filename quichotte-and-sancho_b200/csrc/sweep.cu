@@ -1003,9 +1003,9 @@ static bool dyson_fits(int N) { return dyson_fits_smem(N); }
 
 static bool use_blocked(int N) { return N >= 16 && N <= 128 && (size_t)swz_units(N) * 16 + 1536 <= (size_t)SMEM_MAX; }
 
-static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks) {
+static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks, int variant) {
     const int N = a.N;
-    if (use_blocked(N)) {
+    if (variant == DYSON_BLOCKED && use_blocked(N)) {
         size_t sm = (size_t)swz_units(N) * sizeof(zc);
         QS_CUDA(h, smem_cap((const void *)dyson_bgj));
         a.ws = nullptr;
@@ -1113,7 +1113,13 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         a.iw1 = n;
         a.out_mode = 0;
         a.Gout = h->d_G;
-        if ((rc = launch_dyson(h, a, std::min(n, 148 * 16)))) return rc;
+        {
+            const int cand[2] = {DYSON_BLOCKED, DYSON_UNBLOCKED};
+            const bool two = use_blocked(N);
+            rc = tune_launch(h, TUNE_DYSON, N, two ? cand : cand + 1, two ? 2 : 1, DYSON_BLOCKED,
+                             [&](int v) { return launch_dyson(h, a, std::min(n, 148 * 16), v); });
+            if (rc) return rc;
+        }
         KeldyshArgs k{};
         k.nA = nA;
         k.n = n;
@@ -1131,20 +1137,26 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gRd = h->d_gRd;
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
-        int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
-        int pi;
+        const int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
         const int nbt = std::min(n, 148);
-        if (nA >= 48 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt)) {
-            QS_CUDA(h, smem_cap((const void *)keldysh_tc));
-            pi = prof_begin(h, K_KELDYSH);
-            keldysh_tc<<<nbt, 256, KD_SMEM, h->stream>>>(k);
-        } else {
-            pi = prof_begin(h, K_KELDYSH);
-            keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
-        }
-        prof_end(h, pi);
-        QS_CUDA(h, cudaGetLastError());
-        return 0;
+        auto launch_k = [&](int v) -> int {
+            int pi;
+            if (v == KELDYSH_TC) {
+                QS_CUDA(h, smem_cap((const void *)keldysh_tc));
+                pi = prof_begin(h, K_KELDYSH);
+                keldysh_tc<<<nbt, 256, KD_SMEM, h->stream>>>(k);
+            } else {
+                pi = prof_begin(h, K_KELDYSH);
+                keldysh_scf2<<<nb, 256, 0, h->stream>>>(k);
+            }
+            prof_end(h, pi);
+            QS_CUDA(h, cudaGetLastError());
+            return 0;
+        };
+        const int cand[2] = {KELDYSH_TC, KELDYSH_CUDA};
+        const bool tc_ok = nA >= 32 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt);
+        return tune_launch(h, TUNE_KELDYSH, nA, tc_ok ? cand : cand + 1, tc_ok ? 2 : 1,
+                           (tc_ok && nA >= 48) ? KELDYSH_TC : KELDYSH_CUDA, launch_k);
     }
     // chunked full inversion + per-energy outputs
     const int Mrows = (mode == M_FINAL) ? N : nA;
@@ -1154,7 +1166,7 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         a.iw1 = iw1;
         a.out_mode = 1;
         a.Gout = h->d_G;
-        if ((rc = launch_dyson(h, a, std::min(iw1 - iw0, 148 * 16)))) return rc;
+        if ((rc = launch_dyson(h, a, std::min(iw1 - iw0, 148 * 16), DYSON_BLOCKED))) return rc;
         FinalArgs f{};
         f.N = N;
         f.nS = h->nS;

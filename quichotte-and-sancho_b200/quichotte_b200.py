@@ -144,7 +144,8 @@ C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current
          "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
          "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
          "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
-         "qs_server_budget_gib", "qs_server_destroy")
+         "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice")
+TUNE_DYSON, TUNE_KELDYSH = 0, 1
 QS_ERR_NOALLOC_LIMIT = -1001
 QS_ERR_TOO_LARGE = -1002
 
@@ -157,6 +158,21 @@ class QsRequestResult(ctypes.Structure):
     _fields_ = ([("id", ctypes.c_int64)] + [(k, ctypes.c_int) for k in ("status", "converged", "n_iter", "n_mixed")]
                 + [(k, ctypes.c_double) for k in ("fmax", "J_up", "J_down", "solve_s", "t_arrival", "t_start",
                                                   "t_done", "device_gib")] + [("error", ctypes.c_char * 160)])
+
+
+_lib.qs_autotune.argtypes = [ctypes.c_int]
+_lib.qs_tuned_choice.argtypes = [ctypes.c_int, ctypes.c_int]
+
+
+def autotune(mode):
+    """1: time kernel variants per size (default); 0: size heuristics; 2/3: force variant
+    1 (tensor-core/blocked) or 2; -1: forget the recorded choices."""
+    if _lib.qs_autotune(mode) != 0:
+        raise ValueError(mode)
+
+
+def tuned_choice(kind, size):
+    return _lib.qs_tuned_choice(kind, size)
 
 
 _lib.qs_estimate_bytes.argtypes = [ctypes.POINTER(QsProblem), _dp]

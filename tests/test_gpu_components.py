@@ -225,3 +225,38 @@ def test_mixed_solve_matches_fp64_solve(case):
     for k in o64:
         a, b_ = np.asarray(omx[k]), np.asarray(o64[k])
         assert np.max(np.abs(a - b_)) <= 1e-6 * max(np.max(np.abs(b_)), 1e-300), k
+
+
+# ---- autotuner: every variant it chooses between computes the same step ----
+
+@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("ions_turns", [(4, 2), (7, 4), (10, 6)])
+def test_forced_kernel_variants_match_oracle(mode, ions_turns):
+    """Blocked/tensor-core (mode 2) and unblocked/CUDA-core (mode 3) Dyson and Keldysh at
+    N = nA = 16, 56, 120: residual within 1e-11 of the oracle."""
+    ni, nt = ions_turns
+    m = qb.Model.helix(N_ions=ni, N_turns=nt, hel_length=0.34 * nt, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                       lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
+                       dw=1.0, up=1.0, delta=0.04, order=2)
+    qb.autotune(mode)
+    try:
+        gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+        x = os_.initial_vector(0.2) + 1e-3 * np.random.default_rng(5).standard_normal(gs.n_vec)
+        Fg, _ = gs.residual(0.2, x)
+        Fo, _ = os_.residual(0.2, x)
+        assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
+    finally:
+        qb.autotune(1)
+
+
+def test_autotuner_records_a_choice_per_size():
+    m = qb.Model.helix(N_ions=7, N_turns=4, hel_length=1.36, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                       lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
+                       dw=1.0, up=1.0, delta=0.04, order=2)
+    qb.autotune(-1)
+    qb.autotune(1)
+    s = qb.Solver(m)
+    s.residual(0.3, s.initial_vector(0.3))
+    assert s.nA == 56
+    assert qb.tuned_choice(qb.TUNE_DYSON, 56) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, 56) in (1, 2)
+    s.close()
