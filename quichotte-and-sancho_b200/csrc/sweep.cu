@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(512) dyson_gj(DysonArgs a) {
                 v = tid < nw ? wv[tid] : -1.0;
                 vi = tid < nw ? wi[tid] : N;
                 warp_argmax(v, vi);
+                if (vi >= N) vi = k;  // no comparable entry (NaN column): keep row k, in range
                 if (tid == 0) { piv_s = vi; perm[k] = vi; }
             }
             __syncthreads();
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
     zc *M = (zc *)smem_raw;
     // static shared memory stays below 1536 bytes (use_blocked): N = 120 takes the rest
     __shared__ unsigned char perm[128];
-    __shared__ double cand_v[4];
+    __shared__ unsigned long long cand_k[4];  // each panel warp's pivot key (0: no row searched)
     __shared__ int cand_i[4];
     __shared__ zc cand_row[4][GJ_B];  // each panel warp's pivot candidate row (panel part)
     __shared__ zc krow[GJ_B];         // the panel part of row k before the exchange
@@ -304,17 +305,16 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                     // integer warp reductions (high word + 1, 0 for rows not searched; then the
                     // low word among the lanes holding the maximal high word) replace a chain
                     // of FP64 shuffles
+                    // (a NaN is an ordinary large key here, so a pivot row is always found)
                     const double v = valid ? cabs1(R[0]) : 0.0;
                     const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
-                    const unsigned hk = valid ? (unsigned)(bits >> 32) + 1u : 0u, lk = (unsigned)bits;
+                    const unsigned hk = valid ? min((unsigned)(bits >> 32), 0xfffffffeu) + 1u : 0u, lk = (unsigned)bits;
                     const unsigned mh = __reduce_max_sync(0xffffffffu, hk);
                     const unsigned ml = __reduce_max_sync(0xffffffffu, hk == mh ? lk : 0u);
                     const unsigned bal = __ballot_sync(0xffffffffu, valid && hk == mh && lk == ml);
                     const int wl = bal ? __ffs(bal) - 1 : 32;
-                    const double m =
-                        mh ? __longlong_as_double((long long)(((unsigned long long)(mh - 1u) << 32) | ml)) : -1.0;
                     if (lane == 0) {
-                        cand_v[warp] = m;
+                        cand_k[warp] = ((unsigned long long)mh << 32) | ml;
                         cand_i[warp] = bal ? 32 * warp + wl : N;
                     }
                     if (lane == wl) {  // this warp's candidate publishes its scaled row
@@ -326,19 +326,20 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                         for (int j = 0; j < GJ_B; j++) krow[j] = R[j];
                     }
                     panel_bar();
-                    double bv = cand_v[0];
-                    int p = cand_i[0], wb = 0;
+                    // the largest key; on a tie the lower warp (lower rows) wins, as the first
+                    // maximum. The warp holding row k has a key > 0, so p is a row in [k, N).
+                    unsigned long long bk = cand_k[0];
+                    int wb = 0;
 #pragma unroll
                     for (int q = 1; q < 4; q++) {
-                        const double cv = cand_v[q];
-                        const int ci = cand_i[q];
-                        if (cv > bv || (cv == bv && ci < p)) {
-                            bv = cv;
-                            p = ci;
+                        const unsigned long long ck = cand_k[q];
+                        if (ck > bk) {
+                            bk = ck;
                             wb = q;
                         }
                     }
-                    if (bv == 0.0 && !singular) {  // cabs1 of the pivot is zero
+                    const int p = cand_i[wb];
+                    if (bk == (1ull << 32) && !singular) {  // cabs1 of the pivot is +0
                         singular = true;           // every panel thread sees the same pivot
                         if (tid == 0) first_zero_s = k + 1;
                     }

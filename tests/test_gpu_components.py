@@ -260,3 +260,29 @@ def test_autotuner_records_a_choice_per_size():
     assert s.nA == 56
     assert qb.tuned_choice(qb.TUNE_DYSON, 56) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, 56) in (1, 2)
     s.close()
+
+
+# ---- failure detection: SCF runaway, as scf_residual2 + check_diag_sanity ----
+
+@pytest.mark.parametrize("ions", [3, 4])
+@pytest.mark.parametrize("stride", [7, 1])
+def test_runaway_state_aborts_like_the_oracle(stride, ions):
+    """A state holding NaNs (every 7th entry, or all) makes the residual report abort
+    (src/scf.f90:180-186 via the NaN test of common/scf_checks.f90:59-91) and zero F, on the
+    GPU as in the oracle. The Dyson kernels keep every pivot row in range for NaN columns,
+    and a normal residual follows on the same handle. N = 12 takes the unblocked Gauss-Jordan
+    kernel, N = 16 the blocked one."""
+    m = small_helix(0.05) if ions == 3 else qb.Model.helix(
+        N_ions=4, N_turns=2, hel_length=0.6, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0, lamb=0.01, U_int=1.0,
+        GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0, dw=1.0, up=1.0, delta=0.04, order=2)
+    gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+    x0 = os_.initial_vector(0.3)
+    x = x0.copy()
+    x[::stride] = np.nan
+    Fg, ag = gs.residual(0.3, x)
+    Fo, ao = os_.residual(0.3, x)
+    assert ag and ao
+    assert not np.any(Fg) and not np.any(Fo)
+    Fg2, ag2 = gs.residual(0.3, x0)
+    Fo2, _ = os_.residual(0.3, x0)
+    assert not ag2 and np.max(np.abs(Fg2 - Fo2)) < 1e-11
