@@ -5,8 +5,9 @@
 // tensor-core or CUDA-core GEMMs). The first launch of a step at a size not yet in the table
 // times every candidate on the handle's own inputs (CUDA events on its stream) and records
 // the fastest; later launches at that size, from any handle of the process, use the
-// recorded choice. Every candidate computes the same step, so the outputs of the timed
-// launches are interchangeable.
+// recorded choice. Every candidate computes the same step; the chosen one is launched last,
+// so the step's output is always the recorded variant's (bit-identical results whether or
+// not this launch did the tuning).
 #include <map>
 #include <mutex>
 #include <utility>
@@ -75,7 +76,9 @@ int tune_launch(qs_handle *h, int kind, int size, const int *cand, int ncand, in
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     tune_put(kind, size, best);
-    return 0;
+    // the step's output comes from the recorded choice, as on every later launch: results
+    // do not depend on when the size was tuned
+    return best == cand[ncand - 1] ? 0 : launch(best);
 }
 
 }  // namespace qs

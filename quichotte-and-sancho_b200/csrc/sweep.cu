@@ -615,6 +615,8 @@ __device__ __forceinline__ void cpa16(void *dst, const void *src, bool valid) {
 // = Bm[k + n nA] staged [n][k]; BT = true: B(k, n) = conj(Bm[n + k nA]) staged [k][n]. Only
 // columns nlo..nhi-1 of B are staged. Every thread of the block calls it (the panel copies);
 // warps with !active skip the MMAs.
+// Tiles that cannot contribute are skipped (warp-uniform): columns or rows beyond nA and,
+// with BT (the upper triangle of G^<), tiles wholly below the diagonal.
 template <int NT, bool BT>
 __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__restrict__ Bm, int nA, int nlo, int nhi,
                                         int m0, int n0, bool active, zc *sm, double (&cr)[2][NT][4],
@@ -668,6 +670,9 @@ __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__re
 #pragma unroll
             for (int ni = 0; ni < NT; ni++) {
                 const int c0 = n0 + 8 * ni;
+                if (c0 >= nA) continue;
+                const bool t0 = m0 < nA && (!BT || m0 <= c0 + 7), t1 = m0 + 16 < nA && (!BT || m0 + 16 <= c0 + 7);
+                if (!t0 && !t1) continue;
                 double br[4], bi[4], nbi[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
@@ -676,18 +681,123 @@ __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__re
                     bi[q] = BT ? -v.y : v.y;
                     nbi[q] = -bi[q];
                 }
-                // the two row tiles interleaved: dependent MMAs are three apart
-                dmma16816(cr[0][ni], ar[0], br);
-                dmma16816(cr[1][ni], ar[1], br);
-                dmma16816(ci[0][ni], ar[0], bi);
-                dmma16816(ci[1][ni], ar[1], bi);
-                dmma16816(cr[0][ni], ai[0], nbi);
-                dmma16816(cr[1][ni], ai[1], nbi);
-                dmma16816(ci[0][ni], ai[0], br);
-                dmma16816(ci[1][ni], ai[1], br);
+                if (t0 && t1) {  // the two row tiles interleaved: dependent MMAs are three apart
+                    dmma16816(cr[0][ni], ar[0], br);
+                    dmma16816(cr[1][ni], ar[1], br);
+                    dmma16816(ci[0][ni], ar[0], bi);
+                    dmma16816(ci[1][ni], ar[1], bi);
+                    dmma16816(cr[0][ni], ai[0], nbi);
+                    dmma16816(cr[1][ni], ai[1], nbi);
+                    dmma16816(ci[0][ni], ai[0], br);
+                    dmma16816(ci[1][ni], ai[1], br);
+                } else if (t0) {
+                    dmma16816(cr[0][ni], ar[0], br);
+                    dmma16816(ci[0][ni], ar[0], bi);
+                    dmma16816(cr[0][ni], ai[0], nbi);
+                    dmma16816(ci[0][ni], ai[0], br);
+                } else {
+                    dmma16816(cr[1][ni], ar[1], br);
+                    dmma16816(ci[1][ni], ar[1], bi);
+                    dmma16816(cr[1][ni], ai[1], nbi);
+                    dmma16816(ci[1][ni], ai[1], br);
+                }
             }
         }
         __syncthreads();  // the stage is refilled two chunks later
+    }
+}
+
+// The upper triangle of G^< = T G^dagger as a list of 16 x 8 tiles (row tile rt, column
+// tile ct with 16 rt <= 8 ct + 7, inside nA): pass p gives warp w the tiles p*64 + 8 s + w,
+// s < 8, so the warps share every pass evenly. Operand panels as in kd_gemm (B conjugate-
+// transposed from G); put(i, j, re, im) receives every element of the warp's tiles.
+constexpr int KD_SLOTS = 8;
+__device__ __forceinline__ int kd_upper_tiles(int nA) {
+    int cnt = 0;
+    for (int ct = 0; 8 * ct < nA; ct++) cnt += min((8 * ct + 7) / 16 + 1, (nA + 15) / 16);
+    return cnt;
+}
+// the t-th upper tile in column-major order of tiles
+__device__ __forceinline__ void kd_upper_tile(int nA, int t, int &rt, int &ct) {
+    for (ct = 0; 8 * ct < nA; ct++) {
+        const int h = min((8 * ct + 7) / 16 + 1, (nA + 15) / 16);
+        if (t < h) {
+            rt = t;
+            return;
+        }
+        t -= h;
+    }
+    rt = -1;
+}
+
+template <class PUT>
+__device__ __forceinline__ void kd_upper_gemm(const zc *__restrict__ T, const zc *__restrict__ G, int nA, zc *sm,
+                                              PUT put) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    const int nk = (nA + 15) / 16, ntl = kd_upper_tiles(nA);
+    for (int base = 0; base < ntl; base += 8 * KD_SLOTS) {
+        int rts[KD_SLOTS], cts[KD_SLOTS];
+#pragma unroll
+        for (int q = 0; q < KD_SLOTS; q++) {
+            const int t = base + 8 * q + warp;
+            if (t < ntl) kd_upper_tile(nA, t, rts[q], cts[q]);
+            else rts[q] = -1;
+        }
+        double cr[KD_SLOTS][4], ci[KD_SLOTS][4];
+#pragma unroll
+        for (int q = 0; q < KD_SLOTS; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) cr[q][e] = ci[q][e] = 0.0;
+        auto load = [&](int kc, int st) {
+            zc *As = sm + st * KD_STAGE, *Bs = As + KD_ASZ;
+            const int k0 = kc * 16;
+            for (int idx = tid; idx < 16 * KD_MP; idx += blockDim.x) {
+                const int m = idx & (KD_MP - 1), kk = idx >> 7;
+                const bool v = m < nA && k0 + kk < nA;
+                cpa16(&As[kk * KD_LDA + m], v ? T + m + (size_t)(k0 + kk) * nA : T, v);
+                cpa16(&Bs[kk * KD_LDA + m], v ? G + m + (size_t)(k0 + kk) * nA : G, v);
+            }
+        };
+        load(0, 0);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        for (int kc = 0; kc < nk; kc++) {
+            if (kc + 1 < nk) load(kc + 1, (kc + 1) & 1);
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            __syncthreads();
+            const zc *As = sm + (kc & 1) * KD_STAGE, *Bs = As + KD_ASZ;
+#pragma unroll
+            for (int q = 0; q < KD_SLOTS; q++) {
+                if (rts[q] < 0) continue;
+                const int r0 = 16 * rts[q], c0 = 8 * cts[q];
+                double ar[8], ai[8], br[4], bi[4], nbi[4];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const zc v = As[(t4 + 4 * (e >> 1)) * KD_LDA + r0 + g + 8 * (e & 1)];
+                    ar[e] = v.x;
+                    ai[e] = v.y;
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const zc v = Bs[(t4 + 4 * e) * KD_LDA + c0 + g];  // B(k, n) = conj(G(n, k))
+                    br[e] = v.x;
+                    bi[e] = -v.y;
+                    nbi[e] = v.y;
+                }
+                dmma16816(cr[q], ar, br);
+                dmma16816(ci[q], ar, bi);
+                dmma16816(cr[q], ai, nbi);
+                dmma16816(ci[q], ai, br);
+            }
+            __syncthreads();  // the stage is refilled two chunks later
+        }
+#pragma unroll
+        for (int q = 0; q < KD_SLOTS; q++) {
+            if (rts[q] < 0) continue;
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                put(16 * rts[q] + g + 8 * (e >> 1), 8 * cts[q] + 2 * t4 + (e & 1), cr[q][e], ci[q][e]);
+        }
     }
 }
 
@@ -755,32 +865,8 @@ __global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
                 if (a.gLd) a.gLd[(size_t)iw * nA + r] = zc{vr, vi};
             }
         };
-        // upper triangle of G^< = T G^dagger: warp w takes the 32 x 32 block (bi, bj) =
-        // (0,0) (0,1) (1,1) (0,2) (1,2) (2,2) (0,3) (1,3) ...
-        {
-            const int bi = (0x10210100 >> (4 * warp)) & 15, bj = (0x33222110 >> (4 * warp)) & 15;
-            double cr[2][4][4], ci[2][4][4];
-            const int m0 = 32 * bi, n0 = 32 * bj;
-            kd_gemm<4, true>(T, G, nA, 0, min(nA, KD_MP), m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
-#pragma unroll
-            for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-                for (int ni = 0; ni < 4; ni++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        put(m0 + 16 * mi + g + 8 * (q >> 1), n0 + 8 * ni + 2 * t4 + (q & 1), cr[mi][ni][q], ci[mi][ni][q]);
-        }
-        // ... and (2,3), (3,3) as 32 x 8 strips, four warps each
-        if (nA > 96) {
-            double cr[2][1][4], ci[2][1][4];
-            const int m0 = 32 * (2 + (warp >> 2)), n0 = 96 + 8 * (warp & 3);
-            kd_gemm<1, true>(T, G, nA, 96, KD_MP, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
-#pragma unroll
-            for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    put(m0 + 16 * mi + g + 8 * (q >> 1), n0 + 2 * t4 + (q & 1), cr[mi][0][q], ci[mi][0][q]);
-        }
+        // upper triangle of G^< = T G^dagger, 16 x 8 tiles shared evenly by the warps
+        kd_upper_gemm(T, G, nA, sm, put);
         // G^r part of the block (8 elements a thread in flight)
         for (int base = threadIdx.x; base < nfull; base += 8 * blockDim.x) {
             zc gv[8];
