@@ -41,11 +41,11 @@ N_OMEGA, W_LO, W_HI = 16384, -12.0, 12.0
 VOLTS = [round(-1.0 + 0.05 * k, 10) for k in range(41)]
 
 
-def model_cfg1(qb, n_omega=N_OMEGA):
+def model_cfg1(qb, n_omega=N_OMEGA, ions=N_IONS, turns=N_TURNS):
     """Helix model with its grid exactly on [W_LO, W_HI] with n_omega points
     (omega_i = w_init + i*delta, i = 1..n; w_init = Ev_min - dw, n = int((w_fin-w_init)/delta))."""
-    hel_length = PITCH * N_TURNS * (N_IONS - 1) / N_IONS  # dz = pitch / N_ions
-    args = dict(N_ions=N_IONS, N_turns=N_TURNS, hel_length=hel_length, hel_radius=RADIUS, hand=1.0, E_CC=0.0,
+    hel_length = PITCH * turns * (ions - 1) / ions  # dz = pitch / N_ions
+    args = dict(N_ions=ions, N_turns=turns, hel_length=hel_length, hel_radius=RADIUS, hand=1.0, E_CC=0.0,
                 t_hop=1.0, lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0)
     probe = qb.Model.helix(dw=1.0, up=1.0, delta=0.1, **args)
     ev = np.linalg.eigvalsh(probe.H)
@@ -248,6 +248,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=4096)
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
     ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
+    ap.add_argument("--helix", default=f"{N_IONS}x{N_TURNS}", help="sites/turn x turns; other sizes for profiling only")
     ap.add_argument("--serve", type=int, default=16,
                     help="requests of the serving stream (0: none; the full stream is 512)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrivals per second")
@@ -271,7 +272,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
 
-    m = model_cfg1(qb, args.n_omega)
+    ions, turns = (int(v) for v in args.helix.split("x"))
+    m = model_cfg1(qb, args.n_omega, ions, turns)
     block = voltage_block(rank, world)
     seq = [block[k % len(block)] for k in range(args.warmup + args.steps)]
     fresh = [k == 0 or (k % len(block) == 0) for k in range(len(seq))]
@@ -363,7 +365,7 @@ def main():
             "unit": "IV points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if prec_name == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": f"helix 10x6 (120x120 complex), {n} energies on [-12,12] eV, order 2, U=1.0 eV, "
+            "config": {"workload": f"helix {ions}x{turns} ({N}x{N} complex), {n} energies on [-12,12] eV, order 2, U=1.0 eV, "
                                    "V sweep -1..1 V step 0.05 with continuation", "precision": prec_name, "nhist": args.nhist,
                        "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 (no flush needed)",
                        "scf_steps_per_point": iters, "converged_points": n_conv},

@@ -34,6 +34,32 @@ template <typename T> __device__ __forceinline__ cplx<T> twid(const cplx<T> *tw,
     return sign < 0 ? tw[m] : conj(tw[m]);
 }
 
+// an FP64 twiddle at the kernel's element type
+template <typename T> __device__ __forceinline__ cplx<T> cvt(zc v) { return cplx<T>{(T)v.x, (T)v.y}; }
+
+// The shared-memory twiddle table of a length-L transform. Power-of-two lengths 64/128/256:
+// the twiddles of each pass with Ns > 1 laid out [r][k] (W_L^{r k L/(Ns R)} at r Ns + k,
+// pass Ns = 8 first, then Ns = 64), so that the lanes of a pass read consecutive entries;
+// other lengths: twL[m] = W_L^m.
+__host__ __device__ __forceinline__ int fft_table_len(int L) {
+    return L == 64 ? 64 : (L == 128 ? 192 : (L == 256 ? 320 : L));
+}
+// fill it from the FP64 table of W_Nf (tw[m * tws] = W_L^m), all threads of the block
+template <typename T> __device__ void fft_table_fill(cplx<T> *tbl, int L, const zc *__restrict__ tw, int tws) {
+    if (L == 64 || L == 128 || L == 256) {
+        for (int idx = threadIdx.x; idx < 64; idx += blockDim.x) {
+            const int r = idx >> 3, k = idx & 7;
+            tbl[idx] = cvt<T>(tw[(size_t)(r * k * (L / 64)) * tws]);
+        }
+        for (int idx = threadIdx.x; idx < L; idx += blockDim.x) {  // (L / 64) x 64
+            const int r = idx >> 6, k = idx & 63;
+            if (L > 64) tbl[64 + idx] = cvt<T>(tw[(size_t)(r * k) * tws]);
+        }
+    } else {
+        for (int m = threadIdx.x; m < L; m += blockDim.x) tbl[m] = cvt<T>(tw[(size_t)m * tws]);
+    }
+}
+
 // multiply by sign*i
 template <typename T> __device__ __forceinline__ cplx<T> mul_si(cplx<T> a, int sign) {
     return sign < 0 ? cplx<T>{a.y, -a.x} : cplx<T>{-a.y, a.x};
@@ -164,9 +190,9 @@ __device__ void warp_fft(cplx<T> *s, cplx<T> *scratch, const FftLen &P, int sign
 // ---------------------------------------------------------------------------------
 template <typename T, int L, int R, int Ns>
 __device__ __forceinline__ void pow2_pass(cplx<T> *s, int ps, int nvalid, int sign, const cplx<T> *twL) {
+    static_assert(Ns == 1 || Ns == 8 || Ns == 64, "the passes of warp_fft_pow2");
     constexpr int nR = L / R;  // butterflies per sequence
     constexpr int U = 8 / R;   // butterflies per lane
-    constexpr int ang = L / (Ns * R);
     const int lane = threadIdx.x & 31;
     cplx<T> v[U][R];
 #pragma unroll
@@ -182,8 +208,9 @@ __device__ __forceinline__ void pow2_pass(cplx<T> *s, int ps, int nvalid, int si
         const int b = lane + 32 * u, sq = b / nR, j = b % nR;
         const int k = j % Ns;
         if (Ns > 1 && k) {
+            constexpr int off = (Ns == 8) ? 0 : 64;  // this pass's part of the table ([r][k])
 #pragma unroll
-            for (int r = 1; r < R; r++) v[u][r] = v[u][r] * twid(twL, r * k * ang, sign);
+            for (int r = 1; r < R; r++) v[u][r] = v[u][r] * twid(twL, off + r * Ns + k, sign);
         }
         dft<T, R>(v[u], sign, twL, L);
         cplx<T> *x = s + sq * ps;
@@ -208,7 +235,8 @@ __device__ __forceinline__ void warp_fft_pow2(cplx<T> *s, int ps, int nvalid, in
 __host__ __device__ __forceinline__ int fft_group(int L) { return (L == 64 || L == 128 || L == 256) ? 256 / L : 1; }
 
 // Transform the group of up to fft_group(L) sequences at s + q ps (q < nvalid) by the
-// calling warp; scratch is used by the generic path (one sequence per call).
+// calling warp with the table of fft_table_fill; scratch is used by the generic path (one
+// sequence per call).
 template <typename T>
 __device__ __forceinline__ void warp_fft_group(cplx<T> *s, int ps, int nvalid, cplx<T> *scratch, const FftLen &P,
                                                int sign, const cplx<T> *twL) {

@@ -26,9 +26,6 @@
 
 namespace qs {
 
-// an FP64 twiddle at the kernel's element type
-template <typename T> __device__ __forceinline__ cplx<T> cvt(zc v) { return cplx<T>{(T)v.x, (T)v.y}; }
-
 // ---------------------------------------------------------------------------------
 // Kernel A: forward length-N1 transforms of the zero-padded element sequences.
 // Block tile: SA adjacent sequences x GA adjacent m2 (SA*16 B contiguous per energy block
@@ -48,8 +45,8 @@ __global__ void __launch_bounds__(256, 2) sig2_fwdA(const double *__restrict__ X
     const int nseq = SA * GA;
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
-    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
+    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // the length-N1 table
+    fft_table_fill(twL, N1, tw, N2);
     // only m1 < ceil((n - m2)/N2) can be non-zero (zero padding beyond n energies)
     const int m1max = (n + N2 - 1) / N2;
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
@@ -208,9 +205,9 @@ __global__ void __launch_bounds__(512) sig2_mid(const cplx<T> *__restrict__ Y, c
     cplx<T> *O = S0 + 48 * PL;          // 32 sequences: [((stage*2 + b)*2 + ci)*4 + e]
     cplx<T> *scr = O + 32 * PL + (threadIdx.x >> 5) * PL;  // this warp's scratch
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    cplx<T> *twL = O + (32 + nw) * PL;  // W_N2^m, m < N2
-    cplx<T> *twc = twL + N2;            // W_Nf^{m2 col} of the item's two columns
-    for (int m = threadIdx.x; m < N2; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N1]);
+    cplx<T> *twc = O + (32 + nw) * PL;  // W_Nf^{m2 col} of the item's two columns
+    cplx<T> *twL = twc + 2 * N2;        // the length-N2 table
+    fft_table_fill(twL, N2, tw, N1);
     const int G = fft_group(N2);
 
     if (blockIdx.x < nitems) mid_load<T, N2C>(Y, S0, blockIdx.x, ncp, pairs, nA, fp, PL);
@@ -359,8 +356,8 @@ __global__ void __launch_bounds__(256, 2) sig2_invC(const cplx<T> *__restrict__ 
     }
     cplx<T> *buf = (cplx<T> *)smem_raw;
     cplx<T> *scr = buf + (size_t)nseq * PL + (size_t)(threadIdx.x >> 5) * PL;  // this warp's scratch
-    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
+    cplx<T> *twL = buf + (size_t)(nseq + (blockDim.x >> 5)) * PL;               // the length-N1 table
+    fft_table_fill(twL, N1, tw, N2);
     for (int t = threadIdx.x; t < nseq * N1; t += blockDim.x) {
         int gl = t % GC, r = t / GC;
         int sl = r % 4, l1 = r / 4;
@@ -424,8 +421,8 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
     zc *stg0 = (zc *)smem_raw;      // 2 x NS staging sequences
     zc *twc0 = stg0 + 2 * NS * PL;  // 2 x W_Nf^{m2 l1} of a tile's four columns, [l1][m2 - m20]
     cplx<T> *wb = F64 ? nullptr : (cplx<T> *)(twc0 + 2 * GA * N1);          // FP32 work sequences
-    cplx<T> *twL = F64 ? (cplx<T> *)(twc0 + 2 * GA * N1) : wb + NS * PL;    // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
+    cplx<T> *twL = F64 ? (cplx<T> *)(twc0 + 2 * GA * N1) : wb + NS * PL;    // the length-N1 table
+    fft_table_fill(twL, N1, tw, N2);
     // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores);
     // blockDim.x is a multiple of 16, so a thread keeps its (sequence, m2) on every tile
     const int gl_t = threadIdx.x & 3, sl_t = (threadIdx.x >> 2) & 3;
@@ -502,8 +499,8 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const cplx<T> *__restrict_
     const int nmt = N2 / GC, nfull = nA * nA;
     const int m1max = (n + N2 - 1) / N2;
     cplx<T> *buf0 = (cplx<T> *)smem_raw;
-    cplx<T> *twL = buf0 + 2 * NS * PL;  // W_N1^m, m < N1
-    for (int m = threadIdx.x; m < N1; m += blockDim.x) twL[m] = cvt<T>(tw[(size_t)m * N2]);
+    cplx<T> *twL = buf0 + 2 * NS * PL;  // the length-N1 table
+    fft_table_fill(twL, N1, tw, N2);
     auto tile = [&](int it, int &io, int &jo, int &bb, int &m20, double &c) {
         const int pc = it / nmt;
         m20 = (it % nmt) * GC;
@@ -637,19 +634,20 @@ template <typename T> static InvCPFn<T> pick_invC_p(int N1) {
 template <typename T> static size_t smem_fwdA_p(int N1) {
     const size_t PL = padded_len(N1);
     return sizeof(zc) * (2 * 16 * PL + 2 * 4 * (size_t)N1) + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * 16 * PL) +
-           sizeof(cplx<T>) * N1;
+           sizeof(cplx<T>) * fft_table_len(N1);
 }
 template <typename T> static size_t smem_invC_p(int N1) {
-    return sizeof(cplx<T>) * ((size_t)2 * 16 * padded_len(N1) + (size_t)N1);
+    return sizeof(cplx<T>) * ((size_t)2 * 16 * padded_len(N1) + (size_t)fft_table_len(N1));
 }
 template <typename T> static size_t smem_A(const qs_handle *h) {
-    return sizeof(cplx<T>) * ((size_t)(h->sig2_SA * h->sig2_GA + 8) * padded_len(h->fft.N1) + h->fft.N1);
+    return sizeof(cplx<T>) * ((size_t)(h->sig2_SA * h->sig2_GA + 8) * padded_len(h->fft.N1) + fft_table_len(h->fft.N1));
 }
 template <typename T> static size_t smem_B(const qs_handle *h) {
-    return sizeof(cplx<T>) * ((size_t)(2 * 24 + 32 + 16) * padded_len(h->fft.N2) + 3 * h->fft.N2);
+    return sizeof(cplx<T>) *
+           ((size_t)(2 * 24 + 32 + 16) * padded_len(h->fft.N2) + 2 * h->fft.N2 + fft_table_len(h->fft.N2));
 }
 template <typename T> static size_t smem_C(const qs_handle *h) {
-    return sizeof(cplx<T>) * ((size_t)(4 * h->sig2_GC + 8) * padded_len(h->fft.N1) + h->fft.N1);
+    return sizeof(cplx<T>) * ((size_t)(4 * h->sig2_GC + 8) * padded_len(h->fft.N1) + fft_table_len(h->fft.N1));
 }
 // the persistent forms need N2 a multiple of the 4-column tile (true for N2 >= 64 here)
 static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p<double>(fp.N1) && fp.N2 % 4 == 0; }
