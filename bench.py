@@ -249,6 +249,8 @@ def main():
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
     ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
     ap.add_argument("--helix", default=f"{N_IONS}x{N_TURNS}", help="sites/turn x turns; other sizes for profiling only")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="1: time kernel variants per size (default); 2/3: force variant 1/2 (profiling only)")
     ap.add_argument("--serve", type=int, default=16,
                     help="requests of the serving stream (0: none; the full stream is 512)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrivals per second")
@@ -272,6 +274,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
 
+    qb.autotune(args.autotune)
     ions, turns = (int(v) for v in args.helix.split("x"))
     m = model_cfg1(qb, args.n_omega, ions, turns)
     block = voltage_block(rank, world)

@@ -189,11 +189,12 @@ void qs_server_destroy(qs_server *s);
 
 /* ---- autotuner (no counterpart in the reference) ----
  * Kernel variants whose relative speed depends on the size (kind 0: Dyson, blocked tensor-
- * core or unblocked Gauss-Jordan, by N; kind 1: Keldysh, tensor-core or CUDA-core GEMMs, by
- * nA) are timed on the first launch at a new size and the fastest is kept for the process.
+ * core or unblocked Gauss-Jordan; kind 1: Keldysh, tensor-core or CUDA-core GEMMs) are timed
+ * on the first launch at a new size and the fastest is kept for the process.
  * qs_autotune(1) tunes (default), qs_autotune(0) uses the size heuristics only, 2 / 3 force
  * variant 1 (tensor-core / blocked) / 2 wherever it applies, qs_autotune(-1) forgets the
- * recorded choices. qs_tuned_choice returns the recorded variant (1 or 2) or -1. */
+ * recorded choices. qs_tuned_choice returns the recorded variant (1 or 2) or -1; a decision
+ * is keyed by size = order + 1024 * floor(log2(n_omega)) (order N for Dyson, nA for Keldysh). */
 int qs_autotune(int mode);
 int qs_tuned_choice(int kind, int size);
 

@@ -232,6 +232,13 @@ int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
 // autotuner (autotune.cu): kinds of decisions and the variants they choose between
 enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1 };
 enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2 };
+// the size key of a decision: the matrix order and the octave of the grid length (how many
+// energies each SM gets changes which variant wins)
+inline int tune_key(int order, int n) {
+    int lg = 0;
+    while ((2 << lg) <= n) lg++;
+    return order + 1024 * lg;
+}
 int tune_get(int kind, int size);
 bool tune_enabled();
 void tune_put(int kind, int size, int choice);

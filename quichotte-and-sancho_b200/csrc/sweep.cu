@@ -1203,7 +1203,7 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         {
             const int cand[2] = {DYSON_BLOCKED, DYSON_UNBLOCKED};
             const bool two = use_blocked(N);
-            rc = tune_launch(h, TUNE_DYSON, N, two ? cand : cand + 1, two ? 2 : 1, DYSON_BLOCKED,
+            rc = tune_launch(h, TUNE_DYSON, tune_key(N, n), two ? cand : cand + 1, two ? 2 : 1, DYSON_BLOCKED,
                              [&](int v) { return launch_dyson(h, a, std::min(n, 148 * 16), v); });
             if (rc) return rc;
         }
@@ -1242,7 +1242,7 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         };
         const int cand[2] = {KELDYSH_TC, KELDYSH_CUDA};
         const bool tc_ok = nA >= 32 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt);
-        return tune_launch(h, TUNE_KELDYSH, nA, tc_ok ? cand : cand + 1, tc_ok ? 2 : 1,
+        return tune_launch(h, TUNE_KELDYSH, tune_key(nA, n), tc_ok ? cand : cand + 1, tc_ok ? 2 : 1,
                            (tc_ok && nA >= 48) ? KELDYSH_TC : KELDYSH_CUDA, launch_k);
     }
     // chunked full inversion + per-energy outputs

@@ -171,6 +171,11 @@ def autotune(mode):
         raise ValueError(mode)
 
 
+def tune_key(order, n_omega):
+    """The size key of an autotuner decision (matrix order and the octave of the grid)."""
+    return order + 1024 * (int(n_omega).bit_length() - 1)
+
+
 def tuned_choice(kind, size):
     return _lib.qs_tuned_choice(kind, size)
 

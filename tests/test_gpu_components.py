@@ -258,7 +258,8 @@ def test_autotuner_records_a_choice_per_size():
     s = qb.Solver(m)
     s.residual(0.3, s.initial_vector(0.3))
     assert s.nA == 56
-    assert qb.tuned_choice(qb.TUNE_DYSON, 56) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, 56) in (1, 2)
+    key = qb.tune_key(56, m.n_omega)
+    assert qb.tuned_choice(qb.TUNE_DYSON, key) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, key) in (1, 2)
     s.close()
 
 
