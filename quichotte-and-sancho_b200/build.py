@@ -43,7 +43,7 @@ def build_host(verbose=False):
     srcs = [os.path.join(HERE, "host", f) for f in ("qs_host.cpp", "qs_main.cpp")]
     lib = os.path.join(OUT, "libqs_host.so")
     if not newer(lib, srcs + [os.path.join(INC, "qs_host.h"), os.path.join(INC, "qsb200.h")]):
-        run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + INC] + srcs + ["-o", lib], verbose)
+        run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I" + INC] + srcs + ["-o", lib], verbose)
     return lib
 
 

@@ -277,8 +277,9 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 
 // The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: the leading steps form the
 // second-order self-energies in FP32 (FFTs, 2x2 algebra and spectra); once max|F| falls
-// below mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the step is
-// redone and the solve continues in FP64. The FP32 self-energies leave a noise floor of
+// below mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the solve
+// continues in FP64 (an FP32 step whose max|F| is already below tolf is redone in FP64
+// first, so that it cannot end the solve). The FP32 self-energies leave a noise floor of
 // about 1e-5 in F on the 120x120 helix, so FP32 steps stop well above it. Convergence
 // (max|F| < tolf) is always judged on an FP64 residual, and the converged state meets the
 // FP64 solve's criterion.
@@ -315,11 +316,14 @@ struct Residual2 : BroydenResidual {
         } else {
             since_best++;
         }
-        if (fmax < h->mixed_switch || since_best >= 5 || iter >= h->maxscf / 2) {
-            fp32 = false;  // redo this step in FP64
-            return eval(d_x, d_F, abort, false);
-        }
         n_mixed++;
+        if (fmax < h->mixed_switch || since_best >= 5 || iter >= h->maxscf / 2) {
+            fp32 = false;  // the next steps are FP64
+            if (fmax < h->tolf) {  // never let an FP32 residual declare convergence: redo it
+                n_mixed--;
+                return eval(d_x, d_F, abort, false);
+            }
+        }
         return 0;
     }
 };

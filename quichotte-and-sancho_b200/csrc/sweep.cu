@@ -611,13 +611,11 @@ __device__ __forceinline__ void cpa16(void *dst, const void *src, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 
-// C(m0 + 0..31, n0 + 0..8NT-1) = A B over k < nA. A: nA x nA column-major. BT = false: B(k, n)
-// = Bm[k + n nA] staged [n][k]; BT = true: B(k, n) = conj(Bm[n + k nA]) staged [k][n]. Only
-// columns nlo..nhi-1 of B are staged. Every thread of the block calls it (the panel copies);
-// warps with !active skip the MMAs.
-// Tiles that cannot contribute are skipped (warp-uniform): columns or rows beyond nA and,
-// with BT (the upper triangle of G^<), tiles wholly below the diagonal.
-template <int NT, bool BT>
+// C(m0 + 0..31, n0 + 0..8NT-1) = A B over k < nA. A: nA x nA column-major; B(k, n) =
+// Bm[k + n nA], staged [n][k]; only columns nlo..nhi-1 of B are staged. Every thread of the
+// block calls it (the panel copies); warps with !active skip the MMAs, and tiles beyond nA
+// are skipped (warp-uniform).
+template <int NT>
 __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__restrict__ Bm, int nA, int nlo, int nhi,
                                         int m0, int n0, bool active, zc *sm, double (&cr)[2][NT][4],
                                         double (&ci)[2][NT][4]) {
@@ -638,15 +636,9 @@ __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__re
             cpa16(&As[kk * KD_LDA + m], v ? A + m + (size_t)(k0 + kk) * nA : A, v);
         }
         for (int idx = tid; idx < 16 * nw; idx += blockDim.x) {
-            if (!BT) {
-                const int kk = idx & 15, nn = nlo + (idx >> 4);
-                const bool v = nn < nA && k0 + kk < nA;
-                cpa16(&Bs[nn * KD_LDN + kk], v ? Bm + (k0 + kk) + (size_t)nn * nA : Bm, v);
-            } else {
-                const int nn = nlo + idx % nw, kk = idx / nw;
-                const bool v = nn < nA && k0 + kk < nA;
-                cpa16(&Bs[kk * KD_LDA + nn], v ? Bm + nn + (size_t)(k0 + kk) * nA : Bm, v);
-            }
+            const int kk = idx & 15, nn = nlo + (idx >> 4);
+            const bool v = nn < nA && k0 + kk < nA;
+            cpa16(&Bs[nn * KD_LDN + kk], v ? Bm + (k0 + kk) + (size_t)nn * nA : Bm, v);
         }
     };
     load(0, 0);
@@ -671,15 +663,15 @@ __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__re
             for (int ni = 0; ni < NT; ni++) {
                 const int c0 = n0 + 8 * ni;
                 if (c0 >= nA) continue;
-                const bool t0 = m0 < nA && (!BT || m0 <= c0 + 7), t1 = m0 + 16 < nA && (!BT || m0 + 16 <= c0 + 7);
+                const bool t0 = m0 < nA, t1 = m0 + 16 < nA;
                 if (!t0 && !t1) continue;
                 double br[4], bi[4], nbi[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    const zc v = BT ? Bs[(t4 + 4 * q) * KD_LDA + c0 + g] : Bs[(c0 + g) * KD_LDN + t4 + 4 * q];
+                    const zc v = Bs[(c0 + g) * KD_LDN + t4 + 4 * q];
                     br[q] = v.x;
-                    bi[q] = BT ? -v.y : v.y;
-                    nbi[q] = -bi[q];
+                    bi[q] = v.y;
+                    nbi[q] = -v.y;
                 }
                 if (t0 && t1) {  // the two row tiles interleaved: dependent MMAs are three apart
                     dmma16816(cr[0][ni], ar[0], br);
@@ -839,7 +831,7 @@ __global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
             if (64 * hh >= nA) break;
             double cr[2][4][4], ci[2][4][4];
             const int m0 = 32 * (warp & 3), n0 = 64 * hh + 32 * (warp >> 2);
-            kd_gemm<4, false>(G, S, nA, 64 * hh, 64 * hh + 64, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
+            kd_gemm<4>(G, S, nA, 64 * hh, 64 * hh + 64, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
 #pragma unroll
             for (int mi = 0; mi < 2; mi++)
 #pragma unroll

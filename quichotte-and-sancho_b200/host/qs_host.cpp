@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <complex>
 #include <cstdarg>
@@ -25,6 +26,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -1089,30 +1091,42 @@ qsh_model *to_c(const Model &m) {
 
 // gfortran list-directed REAL(8): one blank separator + a 25-wide field; G editing with
 // 17 significant digits: F form for 0.1 <= |x| < 1e17 (and for 0), left in the field
-// with 5 trailing blanks; otherwise E form d.dddE+ddd right-aligned.
+// with 5 trailing blanks; otherwise E form d.dddE+ddd right-aligned. The digits come from
+// std::to_chars with a precision, which rounds exactly as printf does, several times
+// faster (a spectral file holds n_omega x Norb numbers per voltage).
+static int pad_right_aligned(char *buf, const char *val, int n, int width, int trail) {
+    int k = 0;
+    buf[k++] = ' ';
+    for (int i = n; i < width; i++) buf[k++] = ' ';
+    std::memcpy(buf + k, val, n);
+    k += n;
+    for (int i = 0; i < trail; i++) buf[k++] = ' ';
+    buf[k] = 0;
+    return k;
+}
+
 int fmt_real(double x, char *buf) {
-    char mant[64];
     if (std::isnan(x)) return std::sprintf(buf, "%26s", "NaN");
     if (std::isinf(x)) return std::sprintf(buf, "%26s", x > 0 ? "Infinity" : "-Infinity");
-    std::snprintf(mant, sizeof mant, "%.16E", x);
-    int e = 0;
-    const char *ep = std::strchr(mant, 'E');
-    if (ep) e = std::atoi(ep + 1);
     char val[64];
     if (x == 0.0) {
-        std::snprintf(val, sizeof val, "%.16f", 0.0);
-        if (std::signbit(x)) { std::memmove(val + 1, val, std::strlen(val) + 1); val[0] = '-'; }
-        return std::sprintf(buf, " %20s     ", val);
+        const char *z = std::signbit(x) ? "-0.0000000000000000" : "0.0000000000000000";
+        return pad_right_aligned(buf, z, (int)std::strlen(z), 20, 5);
     }
+    char mant[48];
+    const auto r = std::to_chars(mant, mant + sizeof mant, x, std::chars_format::scientific, 16);
+    const char *ep = static_cast<const char *>(std::memchr(mant, 'e', r.ptr - mant));
+    int e = 0;
+    std::from_chars(ep[1] == '+' ? ep + 2 : ep + 1, r.ptr, e);
     if (e >= -1 && e < 17) {
-        int dec = 16 - e;
-        std::snprintf(val, sizeof val, "%.*f", dec, x);
-        return std::sprintf(buf, " %20s     ", val);
+        const auto f = std::to_chars(val, val + sizeof val, x, std::chars_format::fixed, 16 - e);
+        return pad_right_aligned(buf, val, (int)(f.ptr - val), 20, 5);
     }
     // E form with a 3-digit exponent
-    std::string m(mant, ep - mant);
-    std::snprintf(val, sizeof val, "%sE%c%03d", m.c_str(), e < 0 ? '-' : '+', std::abs(e));
-    return std::sprintf(buf, " %25s", val);
+    int n = (int)(ep - mant);
+    std::memcpy(val, mant, n);
+    n += std::sprintf(val + n, "E%c%03d", e < 0 ? '-' : '+', std::abs(e));
+    return pad_right_aligned(buf, val, n, 25, 0);
 }
 
 }  // namespace
@@ -1294,16 +1308,27 @@ int qsh_write_atom_texture(FILE *f, const qsh_model *m, double V, const double *
 // src/observables.f90:89-102 (dosd is Norb x n_omega, column-major)
 int qsh_write_spectral(FILE *f, const qsh_model *m, double V, const double *dosd) {
     std::fprintf(f, "# V = %10.5f   columns: V, omega, A_ii for i = 1..Norb\n", V);
-    char b[64];
-    std::string s;
-    for (int iw = 0; iw < m->n_omega; iw++) {
-        s.clear();
-        fmt_real(V, b); s += b;
-        fmt_real(m->omega[iw], b); s += b;
-        for (int i = 0; i < m->Norb; i++) { fmt_real(-2.0 * dosd[i + (size_t)iw * m->Norb], b); s += b; }
-        s += '\n';
-        std::fputs(s.c_str(), f);
-    }
+    // rows are formatted in parallel blocks (n_omega x Norb numbers), then written in order
+    const int nw = m->n_omega;
+    const int nthr = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), nw / 256));
+    std::vector<std::string> part(nthr);
+    auto work = [&](int t) {
+        const int w0 = (int)((int64_t)nw * t / nthr), w1 = (int)((int64_t)nw * (t + 1) / nthr);
+        std::string &s = part[t];
+        s.reserve((size_t)(w1 - w0) * (26 * (m->Norb + 2) + 1));
+        char b[64];
+        for (int iw = w0; iw < w1; iw++) {
+            s.append(b, fmt_real(V, b));
+            s.append(b, fmt_real(m->omega[iw], b));
+            for (int i = 0; i < m->Norb; i++) s.append(b, fmt_real(-2.0 * dosd[i + (size_t)iw * m->Norb], b));
+            s += '\n';
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nthr; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+    for (auto &p : part) std::fwrite(p.data(), 1, p.size(), f);
     std::fputs("\n\n", f);
     std::fflush(f);
     return 0;

@@ -1,6 +1,9 @@
 """The host layer (input.dat, models, grid, output format) against the reference's
 golden files (CPU only)."""
+import ctypes
+import math
 import os
+import random
 
 import numpy as np
 import pytest
@@ -73,3 +76,32 @@ def test_helix_grid_and_hermiticity():
 def test_site_dependent_U():
     m = qb.Model.load(os.path.join(CASES, "order2_lefthanded_siteU"))
     assert list(m.U_site[::2]) == [0.8, 0.6, 0.6, 0.8] and not m.U_site[1::2].any()
+
+
+def _printf_rules(x):
+    """gfortran list-directed REAL(8) layout, written with printf-style formatting."""
+    if x == 0.0:
+        v = "%.16f" % 0.0
+        if math.copysign(1.0, x) < 0:
+            v = "-" + v
+        return " %20s     " % v
+    m = "%.16E" % x
+    e = int(m.split("E")[1])
+    if -1 <= e < 17:
+        return " %20s     " % ("%.*f" % (16 - e, x))
+    return " %25s" % (m.split("E")[0] + "E%s%03d" % ("-" if e < 0 else "+", abs(e)))
+
+
+def test_fast_formatter_matches_the_printf_rules():
+    """qsh_fmt_real (std::to_chars digits) against the same rules written with printf, on
+    random magnitudes and the F/E boundaries, signed zeros and extremes."""
+    rnd = random.Random(3)
+    vals = [rnd.uniform(-1, 1) * 10 ** rnd.uniform(-40, 40) for _ in range(20000)]
+    vals += [0.1, -0.1, 0.09999999999999999, 1e17, -1e17, 9.999999999999998e16, 1.0, 0.0, -0.0, 1e-300, 5e-324,
+             1.7976931348623157e308, 2.5e-7, 123456.789]
+    lib = ctypes.CDLL(qb.HOST_PATH)
+    lib.qsh_fmt_real.argtypes = [ctypes.c_double, ctypes.c_char_p]
+    buf = ctypes.create_string_buffer(64)
+    for x in vals:
+        lib.qsh_fmt_real(x, buf)
+        assert buf.value.decode() == _printf_rules(x), repr(x)
