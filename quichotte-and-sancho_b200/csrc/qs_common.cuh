@@ -230,7 +230,7 @@ int sigma2_setup(qs_handle *h);
 // fp32: FFTs, 2x2 algebra and spectra in FP32 (QS_PREC_MIXED handles), Sigma written in FP64
 int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
 // autotuner (autotune.cu): kinds of decisions and the variants they choose between
-enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1 };
+enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1, TUNE_SIG2_A = 2, TUNE_SIG2_C = 3 };
 enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2 };
 // the size key of a decision: the matrix order and the octave of the grid length (how many
 // energies each SM gets changes which variant wins)

@@ -405,33 +405,35 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Kernel A: tile = 4 adjacent sequences x 4 adjacent m2; tiles ordered sequence-tile fastest.
-// The FP64 values are copied into a staging buffer; with T = float they are converted into
-// a work buffer before the transforms (Y then holds FP32 spectra).
-template <typename T, int N1>
-__global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk, int n,
-                                                      const int2 *__restrict__ desc, int nY, FftPlan fp,
-                                                      const zc *__restrict__ tw, cplx<T> *__restrict__ Y, int nitems) {
-    constexpr int SA = 4, GA = 4, NS = SA * GA;
+// Kernel A: tile = 4 adjacent sequences x GA adjacent m2 (GA = 4: one block of 16 warps per
+// SM; GA = 2: two blocks of 8 warps, whose phases interleave); tiles ordered sequence-tile
+// fastest. The FP64 values are copied into a staging buffer; with T = float they are
+// converted into a work buffer before the transforms (Y then holds FP32 spectra).
+template <typename T, int N1, int GA>
+__global__ void __launch_bounds__(128 * GA, 4 / GA) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk, int n,
+                                                              const int2 *__restrict__ desc, int nY, FftPlan fp,
+                                                              const zc *__restrict__ tw, cplx<T> *__restrict__ Y,
+                                                              int nitems) {
+    constexpr int SA = 4, NS = SA * GA;  // one warp per sequence: blockDim.x = 32 NS
     constexpr bool F64 = sizeof(T) == 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int nst = (nY + SA - 1) / SA;
     const int m1max = (n + N2 - 1) / N2;  // zero padding beyond n energies
     zc *stg0 = (zc *)smem_raw;      // 2 x NS staging sequences
-    zc *twc0 = stg0 + 2 * NS * PL;  // 2 x W_Nf^{m2 l1} of a tile's four columns, [l1][m2 - m20]
+    zc *twc0 = stg0 + 2 * NS * PL;  // 2 x W_Nf^{m2 l1} of a tile's GA columns, [l1][m2 - m20]
     cplx<T> *wb = F64 ? nullptr : (cplx<T> *)(twc0 + 2 * GA * N1);          // FP32 work sequences
     cplx<T> *twL = F64 ? (cplx<T> *)(twc0 + 2 * GA * N1) : wb + NS * PL;    // the length-N1 table
     fft_table_fill(twL, N1, tw, N2);
     // lanes: m2 fastest, then sequence (64-byte global runs, conflict-free shared stores);
-    // blockDim.x is a multiple of 16, so a thread keeps its (sequence, m2) on every tile
-    const int gl_t = threadIdx.x & 3, sl_t = (threadIdx.x >> 2) & 3;
+    // blockDim.x is a multiple of NS, so a thread keeps its (sequence, m2) on every tile
+    const int gl_t = threadIdx.x % GA, sl_t = (threadIdx.x / GA) % SA;
     auto load = [&](int it, zc *b, zc *twc) {
         const int s0 = (it % nst) * SA, m20 = (it / nst) * GA;
         const int s = s0 + sl_t, m2 = m20 + gl_t;
         const int2 d = s < nY ? desc[s] : int2{-1, 0};
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int m1 = t >> 4;
+            const int m1 = t / NS;
             const int64_t w = (int64_t)N2 * m1 + m2;
             zc *dst = b + (sl_t * GA + gl_t) * PL + pidx(m1);
             if (m1 < m1max && s < nY && w < n) {
@@ -448,7 +450,7 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
             }
         }
         for (int t = threadIdx.x; t < GA * N1; t += blockDim.x) {
-            const int g2 = t & 3, l1 = t >> 2;
+            const int g2 = t % GA, l1 = t / GA;
             cp_async16(&twc[t], &tw[(size_t)(m20 + g2) * l1]);
         }
     };
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
         __syncthreads();
         // lanes: m2 fastest, then sequence, then l1
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int gl = t & 3, sl = (t >> 2) & 3, l1 = t >> 4;
+            const int gl = t % GA, sl = (t / GA) % SA, l1 = t / NS;
             const int s = s0 + sl, m2 = m20 + gl;
             if (s < nY) Y[(size_t)s * Nf + (size_t)l1 * N2 + m2] = b[(sl * GA + gl) * PL + pidx(l1)] * cvt<T>(twc[l1 * GA + gl]);
         }
@@ -486,14 +488,15 @@ __global__ void __launch_bounds__(512, 1) sig2_fwdA_p(const double *__restrict__
     }
 }
 
-// Kernel C: tile = one column jo+bb of a 2x2 output block x 4 adjacent m2; tiles ordered m2
-// fastest (neighbouring blocks read neighbouring 64-byte pieces of the same V rows)
-template <typename T, int N1>
-__global__ void __launch_bounds__(512, 1) sig2_invC_p(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
-                                                      zc *__restrict__ SigL, int nA, int nAs, int n,
-                                                      const double *__restrict__ Upair, FftPlan fp,
-                                                      const zc *__restrict__ tw, int nitems) {
-    constexpr int GC = 4, NS = 4 * GC;
+// Kernel C: tile = one column jo+bb of a 2x2 output block x GC adjacent m2 (GC = 4: one
+// block of 16 warps per SM; GC = 2: two blocks of 8 warps); tiles ordered m2 fastest
+// (neighbouring blocks read neighbouring pieces of the same V rows)
+template <typename T, int N1, int GC>
+__global__ void __launch_bounds__(128 * GC, 4 / GC) sig2_invC_p(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
+                                                              zc *__restrict__ SigL, int nA, int nAs, int n,
+                                                              const double *__restrict__ Upair, FftPlan fp,
+                                                              const zc *__restrict__ tw, int nitems) {
+    constexpr int NS = 4 * GC;  // one warp per sequence: blockDim.x = 32 NS
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
     const int nmt = N2 / GC, nfull = nA * nA;
@@ -516,7 +519,7 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const cplx<T> *__restrict_
         tile(it, io, jo, bb, m20, c);
         if (c == 0.0) return;  // src/self_energies.f90:167-171: a zero block, nothing to read
         for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
-            const int gl = t & 3, r = t >> 2, sl = r & 3, l1 = r >> 2;
+            const int gl = t % GC, r = t / GC, sl = r & 3, l1 = r >> 2;
             const int a = sl & 1, st = sl >> 1;
             const size_t sid = (size_t)st * nfull + (io + a) + (size_t)(jo + bb) * nA;
             cp_async_elem(b + (sl * GC + gl) * PL + pidx(l1), V + sid * Nf + (size_t)l1 * N2 + m20 + gl, true);
@@ -541,7 +544,7 @@ __global__ void __launch_bounds__(512, 1) sig2_invC_p(const cplx<T> *__restrict_
         __syncthreads();
         // lanes: row a fastest (32-byte global runs), then m2, then stage (conflict-free reads)
         for (int t = threadIdx.x; t < NS * m1max; t += blockDim.x) {
-            const int a = t & 1, gl = (t >> 1) & 3, st = (t >> 3) & 1, m1 = t >> 4;
+            const int a = t & 1, gl = (t >> 1) % GC, st = (t / (2 * GC)) & 1, m1 = t / NS;
             const int64_t w = (int64_t)N2 * m1 + m20 + gl;
             if (w < n) {
                 cplx<T> v = (c != 0.0) ? b[((st * 2 + a) * GC + gl) * PL + pidx(m1)] : cplx<T>{0, 0};
@@ -587,11 +590,6 @@ using FwdAFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan
 template <typename T> using MidFn = void (*)(const cplx<T> *, cplx<T> *, const int2 *, int, FftPlan, const zc *, int);
 template <typename T>
 using InvCFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
-template <typename T>
-using FwdAPFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, cplx<T> *, int);
-template <typename T>
-using InvCPFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
-
 template <typename T> static FwdAFn<T> pick_fwdA(int N1, int SA, int GA) {
     if (SA == 4 && GA == 4) switch (N1) {
             case 64: return sig2_fwdA<T, 64>;
@@ -615,29 +613,45 @@ template <typename T> static InvCFn<T> pick_invC(int N1, int GC) {
         }
     return sig2_invC<T, 0>;
 }
-template <typename T> static FwdAPFn<T> pick_fwdA_p(int N1) {
+template <typename T>
+using FwdAPFn = void (*)(const double *, int64_t, int, const int2 *, int, FftPlan, const zc *, cplx<T> *, int);
+template <typename T>
+using InvCPFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const double *, FftPlan, const zc *, int);
+// persistent kernels A / C for power-of-two N1; w = 4 (16-sequence tiles, one block per
+// SM) or 2 (8-sequence tiles, two blocks per SM)
+template <typename T> static FwdAPFn<T> pick_fwdA_p(int N1, int w) {
+    if (w == 2) switch (N1) {
+            case 64: return sig2_fwdA_p<T, 64, 2>;
+            case 128: return sig2_fwdA_p<T, 128, 2>;
+            case 256: return sig2_fwdA_p<T, 256, 2>;
+        }
     switch (N1) {
-        case 64: return sig2_fwdA_p<T, 64>;
-        case 128: return sig2_fwdA_p<T, 128>;
-        case 256: return sig2_fwdA_p<T, 256>;
+        case 64: return sig2_fwdA_p<T, 64, 4>;
+        case 128: return sig2_fwdA_p<T, 128, 4>;
+        case 256: return sig2_fwdA_p<T, 256, 4>;
     }
     return nullptr;
 }
-template <typename T> static InvCPFn<T> pick_invC_p(int N1) {
+template <typename T> static InvCPFn<T> pick_invC_p(int N1, int w) {
+    if (w == 2) switch (N1) {
+            case 64: return sig2_invC_p<T, 64, 2>;
+            case 128: return sig2_invC_p<T, 128, 2>;
+            case 256: return sig2_invC_p<T, 256, 2>;
+        }
     switch (N1) {
-        case 64: return sig2_invC_p<T, 64>;
-        case 128: return sig2_invC_p<T, 128>;
-        case 256: return sig2_invC_p<T, 256>;
+        case 64: return sig2_invC_p<T, 64, 4>;
+        case 128: return sig2_invC_p<T, 128, 4>;
+        case 256: return sig2_invC_p<T, 256, 4>;
     }
     return nullptr;
 }
-template <typename T> static size_t smem_fwdA_p(int N1) {
-    const size_t PL = padded_len(N1);
-    return sizeof(zc) * (2 * 16 * PL + 2 * 4 * (size_t)N1) + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * 16 * PL) +
+template <typename T> static size_t smem_fwdA_p(int N1, int w) {
+    const size_t PL = padded_len(N1), ns = 4 * w;
+    return sizeof(zc) * (2 * ns * PL + 2 * (size_t)w * N1) + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * ns * PL) +
            sizeof(cplx<T>) * fft_table_len(N1);
 }
-template <typename T> static size_t smem_invC_p(int N1) {
-    return sizeof(cplx<T>) * ((size_t)2 * 16 * padded_len(N1) + (size_t)fft_table_len(N1));
+template <typename T> static size_t smem_invC_p(int N1, int w) {
+    return sizeof(cplx<T>) * ((size_t)2 * 4 * w * padded_len(N1) + (size_t)fft_table_len(N1));
 }
 template <typename T> static size_t smem_A(const qs_handle *h) {
     return sizeof(cplx<T>) * ((size_t)(h->sig2_SA * h->sig2_GA + 8) * padded_len(h->fft.N1) + fft_table_len(h->fft.N1));
@@ -650,17 +664,18 @@ template <typename T> static size_t smem_C(const qs_handle *h) {
     return sizeof(cplx<T>) * ((size_t)(4 * h->sig2_GC + 8) * padded_len(h->fft.N1) + fft_table_len(h->fft.N1));
 }
 // the persistent forms need N2 a multiple of the 4-column tile (true for N2 >= 64 here)
-static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p<double>(fp.N1) && fp.N2 % 4 == 0; }
+static bool persistent_AC(const FftPlan &fp) { return pick_fwdA_p<double>(fp.N1, 4) && fp.N2 % 4 == 0; }
 
 template <typename T> static int sigma2_attributes(qs_handle *h) {
     const FftPlan &fp = h->fft;
     QS_CUDA(h, smem_cap((const void *)pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA)));
     QS_CUDA(h, smem_cap((const void *)pick_mid<T>(fp.N2)));
     QS_CUDA(h, smem_cap((const void *)pick_invC<T>(fp.N1, h->sig2_GC)));
-    if (persistent_AC(fp)) {
-        QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1)));
-        QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1)));
-    }
+    if (persistent_AC(fp))
+        for (int w : {2, 4}) {
+            QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1, w)));
+            QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1, w)));
+        }
     return 0;
 }
 
@@ -762,18 +777,27 @@ template <typename T> static int sigma2_run(qs_handle *h, const double *d_x) {
     const int nA = h->nA;
     const bool pers = persistent_AC(fp);
     cplx<T> *Y = (cplx<T> *)h->d_Y, *V = (cplx<T> *)h->d_V;
-    int pa = prof_begin(h, K_SIG2A);
+    const int cand[2] = {4, 2};  // tile widths, autotuned per size (results are identical)
+    const int key = tune_key(nA, h->n) + (sizeof(T) == 4 ? 1 << 20 : 0);
     if (pers) {
-        const int nitems = (int)((h->nY + 3) / 4) * (fp.N2 / 4);
-        pick_fwdA_p<T>(fp.N1)<<<std::min(nitems, 148), 512, smem_fwdA_p<T>(fp.N1), h->stream>>>(
-            d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, nitems);
+        int rc = tune_launch(h, TUNE_SIG2_A, key, cand, 2, 4, [&](int w) -> int {
+            const int nitems = (int)((h->nY + 3) / 4) * (fp.N2 / w);
+            int pa = prof_begin(h, K_SIG2A);
+            pick_fwdA_p<T>(fp.N1, w)<<<std::min(nitems, 148 * (4 / w)), 128 * w, smem_fwdA_p<T>(fp.N1, w), h->stream>>>(
+                d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, nitems);
+            prof_end(h, pa);
+            QS_CUDA(h, cudaGetLastError());
+            return 0;
+        });
+        if (rc) return rc;
     } else {
+        int pa = prof_begin(h, K_SIG2A);
         dim3 gA((unsigned)((h->nY + h->sig2_SA - 1) / h->sig2_SA), (unsigned)((fp.N2 + h->sig2_GA - 1) / h->sig2_GA));
         pick_fwdA<T>(fp.N1, h->sig2_SA, h->sig2_GA)<<<gA, 256, smem_A<T>(h), h->stream>>>(
             d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, h->sig2_SA, h->sig2_GA);
+        prof_end(h, pa);
+        QS_CUDA(h, cudaGetLastError());
     }
-    prof_end(h, pa);
-    QS_CUDA(h, cudaGetLastError());
     if (h->sig2_npairs > 0) {
         const int nitems = h->sig2_npairs * (fp.N1 / 2 + 1);
         const int gB = std::min(nitems, 148);  // persistent: one block per SM
@@ -782,18 +806,25 @@ template <typename T> static int sigma2_run(qs_handle *h, const double *d_x) {
         prof_end(h, pb);
         QS_CUDA(h, cudaGetLastError());
     }
-    int pc = prof_begin(h, K_SIG2C);
     if (pers) {
-        const int nitems = 2 * h->nAs * h->nAs * (fp.N2 / 4);
-        pick_invC_p<T>(fp.N1)<<<std::min(nitems, 148), 512, smem_invC_p<T>(fp.N1), h->stream>>>(
-            V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
+        int rc = tune_launch(h, TUNE_SIG2_C, key, cand, 2, 4, [&](int w) -> int {
+            const int nitems = 2 * h->nAs * h->nAs * (fp.N2 / w);
+            int pc = prof_begin(h, K_SIG2C);
+            pick_invC_p<T>(fp.N1, w)<<<std::min(nitems, 148 * (4 / w)), 128 * w, smem_invC_p<T>(fp.N1, w), h->stream>>>(
+                V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
+            prof_end(h, pc);
+            QS_CUDA(h, cudaGetLastError());
+            return 0;
+        });
+        if (rc) return rc;
     } else {
+        int pc = prof_begin(h, K_SIG2C);
         dim3 gC((unsigned)(2 * h->nAs * h->nAs), (unsigned)((fp.N2 + h->sig2_GC - 1) / h->sig2_GC));
         pick_invC<T>(fp.N1, h->sig2_GC)<<<gC, 256, smem_C<T>(h), h->stream>>>(
             V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, h->sig2_GC);
+        prof_end(h, pc);
+        QS_CUDA(h, cudaGetLastError());
     }
-    prof_end(h, pc);
-    QS_CUDA(h, cudaGetLastError());
     return 0;
 }
 
