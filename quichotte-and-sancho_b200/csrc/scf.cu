@@ -281,7 +281,7 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 // continues in FP64 (an FP32 step whose max|F| is already below tolf is redone in FP64
 // first, so that it cannot end the solve). The FP32 self-energies leave a noise floor of
 // about 1e-5 in F on the 120x120 helix, so FP32 steps stop well above it. Convergence
-// (max|F| < tolf) is always judged on an FP64 residual, and the converged state meets the
+// (max|F| < tolf) is always decided on an FP64 residual, and the converged state meets the
 // FP64 solve's criterion.
 struct Residual2 : BroydenResidual {
     qs_handle *h;
