@@ -75,10 +75,12 @@ int tune_launch(qs_handle *h, int kind, int size, const int *cand, int ncand, in
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    tune_put(kind, size, best);
+    tune_put(kind, size, best);  // the first record wins when threads tune a size at once
     // the step's output comes from the recorded choice, as on every later launch: results
-    // do not depend on when the size was tuned
-    return best == cand[ncand - 1] ? 0 : launch(best);
+    // do not depend on when, or by which thread, the size was tuned
+    const int chosen = tune_get(kind, size);
+    const int use = chosen >= 0 ? chosen : best;
+    return use == cand[ncand - 1] ? 0 : launch(use);
 }
 
 }  // namespace qs
