@@ -349,6 +349,12 @@ def main():
             "sig2_invC": ("hbm", 2.0 * nA * nA * Nf * 16.0 + 2.0 * nA * nA * n * 16.0),  # read V, write Sigma
             "broyden": ("hbm", nvec * (64.0 + 12.0 * nh) / 3.0),          # per iteration / 3 launches
         }
+        # DRAM bytes per energy measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
+        # the 120x120 helix with 1024 energies (profiles/dyson_bgj_helix120_n1024.md,
+        # profiles/keldysh_tc_helix120_n1024.md); the traffic of a launch is per energy, so it
+        # scales with the number of energies
+        traffic_per_energy = {"dyson_gj": (236.776192e6 + 183.729152e6) / 1024,
+                              "keldysh_scf2": (1064.643e6 + 800.101376e6) / 1024}
         roof = None
         if fam in work and cnt:
             kind, per_launch = work[fam]
@@ -359,8 +365,11 @@ def main():
             else:
                 achieved, peak, unit = per_launch / t / 1e9, peaks.get("hbm_gbs", 6650.0), "GB/s"
                 src_note = f"hbm_gbs of MEASURED_PEAKS.json ({src})"
+            tpe = traffic_per_energy.get(fam) if (N, nA) == (120, 120) else None
             roof = {"kernel": fam, "bound": kind, "achieved": achieved, "peak": peak, "unit": unit,
-                    "frac": achieved / peak, "traffic": None, "peak_source": src_note,
+                    "frac": achieved / peak, "traffic": tpe * n if tpe else None,
+                    "traffic_note": "DRAM bytes per launch, ncu capture at 1024 energies scaled to the launch" if tpe else None,
+                    "peak_source": src_note,
                     "per_launch_work": per_launch, "launches": cnt, "avg_launch_ms": ms / cnt}
         prec_name = "mixed" if "mixed" in arms else "fp64"
         line = {
