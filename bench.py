@@ -238,6 +238,89 @@ def run_reference(args, rank, world):
     return 0
 
 
+def setup_timing(qb, m, repeats=3):
+    """The set-up's dense linear algebra on the device, through the public entry points with
+    host arrays (copies included), beside LAPACK through numpy on the host cores: the grid
+    eigenproblem of the workload's H (zheev, src/quichotte.f90:79-83) and the Loewdin
+    transform at the size of the 40-atom helicene model (124 orbitals, 248 spin-orbitals;
+    seeded synthetic S = I + perturbation, H0, SOC matrix)."""
+    def best(f):
+        ts = []
+        for _ in range(repeats):
+            t = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t)
+        return 1e3 * min(ts)
+    rng = np.random.default_rng(40)
+    N = 124
+    P = rng.standard_normal((N, N))
+    S = np.eye(N) + 0.05 * (P + P.T) / np.linalg.norm(P + P.T, 2)
+    H0 = rng.standard_normal((N, N))
+    H0 = 0.5 * (H0 + H0.T)
+    X = rng.standard_normal((2 * N, 2 * N)) + 1j * rng.standard_normal((2 * N, 2 * N))
+    Lam = 0.005 * (X + X.conj().T)
+
+    def lowdin_numpy():
+        ev, U = np.linalg.eigh(S)
+        W = U / np.sqrt(np.sqrt(ev))
+        Sx2, Sm2 = np.kron(S, np.eye(2)), np.kron(W @ W.T, np.eye(2))
+        Hn = Sm2 @ (np.kron(H0, np.eye(2)) + 0.5 * (Sx2 @ Lam + Lam @ Sx2)) @ Sm2
+        return 0.5 * (Hn + Hn.conj().T)
+    E, _, info = qb.hermitian_eigensystem(m.H)
+    Hd, _ = qb.dftb_lowdin(S, H0, Lam, True)
+    Hn = lowdin_numpy()
+    return {"eigensystem_ms": best(lambda: qb.hermitian_eigensystem(m.H)),
+            "eigensystem_numpy_ms": best(lambda: np.linalg.eigh(m.H)),
+            "eigensystem_rel_err": float(np.max(np.abs(E - np.linalg.eigvalsh(m.H))) / np.max(np.abs(E))),
+            "lowdin_ms": best(lambda: qb.dftb_lowdin(S, H0, Lam, True)), "lowdin_numpy_ms": best(lowdin_numpy),
+            "lowdin_rel_err": float(np.max(np.abs(Hd - Hn)) / np.max(np.abs(Hn))),
+            "workload": f"eigenproblem of the {m.Norb}x{m.Norb} H; Loewdin at N=124 (248 spin-orbitals); "
+                        f"host arrays, best of {repeats}; numpy = LAPACK on the host cores"}
+
+
+def setup_scan(qb):
+    """Sizes and batches of the device set-up beside LAPACK (numpy) on the host cores: random
+    Hermitian matrices (seeded) for the eigenproblem, seeded S = I + perturbation, H0 and SOC
+    matrix for the Loewdin transform. Wall times through the public API with host arrays."""
+    rng = np.random.default_rng(0)
+
+    def herm(N):
+        X = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+        return (X + X.conj().T) / 2
+
+    def wall(f):
+        t = time.perf_counter()
+        r = f()
+        return r, time.perf_counter() - t
+    qb.hermitian_eigensystem(herm(16))  # context and graph code paths once
+    out = {}
+    for N, batch in [(120, 1), (120, 64), (248, 1), (248, 16), (512, 1), (1024, 1), (2048, 1)]:
+        A = np.stack([herm(N) for _ in range(batch)])
+        (E, _, info), tg = wall(lambda: qb.hermitian_eigensystem(A))
+        (En, _), tc = wall(lambda: np.linalg.eigh(A))
+        out[f"eigensystem_N{N}_batch{batch}"] = {"device_s": tg, "numpy_s": tc, "info": int(np.max(info)),
+                                                 "rel_err": float(np.max(np.abs(E - En)) / np.max(np.abs(En)))}
+    for N in (124, 1024):
+        P = rng.standard_normal((N, N))
+        S = np.eye(N) + 0.05 * (P + P.T) / np.linalg.norm(P + P.T, 2)
+        H0 = rng.standard_normal((N, N))
+        H0 = 0.5 * (H0 + H0.T)
+        X = rng.standard_normal((2 * N, 2 * N)) + 1j * rng.standard_normal((2 * N, 2 * N))
+        Lam = 0.005 * (X + X.conj().T)
+
+        def ref():
+            ev, U = np.linalg.eigh(S)
+            W = U / np.sqrt(np.sqrt(ev))
+            Sx2, Sm2 = np.kron(S, np.eye(2)), np.kron(W @ W.T, np.eye(2))
+            Hn = Sm2 @ (np.kron(H0, np.eye(2)) + 0.5 * (Sx2 @ Lam + Lam @ Sx2)) @ Sm2
+            return 0.5 * (Hn + Hn.conj().T)
+        (H, _), tg = wall(lambda: qb.dftb_lowdin(S, H0, Lam, True))
+        Hn, tc = wall(ref)
+        out[f"lowdin_N{N}"] = {"device_s": tg, "numpy_s": tc,
+                               "rel_err": float(np.max(np.abs(H - Hn)) / np.max(np.abs(Hn)))}
+    return {"setup_scan": out, "numpy_threads": os.cpu_count()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -257,8 +340,14 @@ def main():
     ap.add_argument("--serve-inflight", type=int, default=4, help="solves on the device at once")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="both: the FP64 form, then the mixed form (headline value), with their ratio")
+    ap.add_argument("--setup-scan", action="store_true",
+                    help="time the device set-up (eigenproblem, Loewdin) over sizes against LAPACK, print, exit")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.setup_scan:
+        import quichotte_b200 as qb
+        print(json.dumps(setup_scan(qb)), flush=True)
+        return 0
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -408,6 +497,8 @@ def main():
                                            "helices, sites/turn 3-12, turns 1-8, U 0.2-1.5 eV, V -1..1 V, 4096-32768 "
                                            "energies, Poisson arrivals; one fresh-start IV point per request, FP64, "
                                            "Broyden nhist 8; requests above the HBM budget are refused")
+        if world == 1:
+            line["setup"] = setup_timing(qb, m)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(args.ref_sample)
         print(json.dumps(line), flush=True)

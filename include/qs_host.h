@@ -56,6 +56,11 @@ typedef struct qsh_model {
 /* Read <dir>/input.dat (or inputSOC.dat) and build the model. Returns 0, or 1 with
  * the reference's error message in errbuf. Warnings go to `log` if non-NULL. */
 int qsh_load(const char *dir, qsh_model **out, char *errbuf, int errlen, FILE *log);
+/* qsh_load with the set-up linear algebra of `api` where it provides it, on CUDA device
+ * `device` (api NULL: qsh_load). The solver API type is declared below. */
+struct qsh_solver_api;
+int qsh_load_with(const char *dir, const struct qsh_solver_api *api, int device, qsh_model **out, char *errbuf,
+                  int errlen, FILE *log);
 void qsh_free(qsh_model *m);
 
 /* Synthetic helix model without an input file (the input.dat keys of a helix run). */
@@ -91,6 +96,11 @@ typedef struct qsh_solver_api {
     int (*solve_scf)(void *h, double Volt, int fresh_start, qs_scf_result *res);
     int (*current)(void *h, double Volt, double *J_up, double *J_down);
     int (*get_observables)(void *h, double *G_less_obs, double *dosd, double *trU, double *trD);
+    /* optional: the set-up's dense linear algebra (qs_hermitian_eigensystem, qs_dftb_lowdin
+     * of qsb200.h); NULL uses the host's own (cyclic Jacobi and plain products) */
+    int (*hermitian_eigensystem)(int N, int batch, double *A, double *E, int *info, int device);
+    int (*dftb_lowdin)(int N, const double *S, const double *H0, const double *Lam, int soc_dual, double *H,
+                       double *evmin, int device);
 } qsh_solver_api;
 
 /* The program QUICHOTTE (src/quichotte.f90:31-166) on <dir>: reads input.dat, runs

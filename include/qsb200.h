@@ -114,6 +114,30 @@ int qs_self_energies(qs_handle *h, const double *x, double *SigR2, double *SigL2
  * if pivot k of matrix b is zero (the reference's ZGETRF INFO > 0). */
 int qs_invert_batched(int N, int batch, double *A, int *info, int precision);
 
+/* ---- set-up (host arrays; each call allocates and frees its own device buffers and runs
+ * on CUDA device `device`, or on the calling thread's current device if device < 0) ---- */
+
+/* hermitian_eigensystem (common/linear_algebra.f90:32-56, LAPACK zheev) over a batch: A holds
+ * `batch` N x N Hermitian complex column-major matrices (only their Hermitian part is used;
+ * the diagonal's imaginary part is ignored) and is replaced by the eigenvectors, one per
+ * column, in the order of E (`batch` x N eigenvalues, ascending). Parallel two-sided Jacobi on
+ * the device. info[b] = 0, or 1 if matrix b did not converge or holds non-finite entries
+ * (the reference's ZHEEV INFO > 0, where it stops). 1 <= N <= 2048, batch <= 65535. Returns 0,
+ * 1 if some info[b] != 0, -1 for bad arguments, or a CUDA error (< 0). */
+int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, int device);
+
+/* The dense linear algebra of build_hamiltonian_from_dftb_hs (src/hamiltonian.f90:625-689):
+ * S (N x N real symmetric overlap) and H0 (N x N real, eV) as the reference holds them after
+ * symmetrisation, Lam (2N x 2N complex, the p-shell SOC matrix, spin fastest);
+ *   S^-1/2 = U diag(s^-1/2) U^T from the eigenpairs of S,
+ *   Hao = H0 (x) I2 + (soc_dual ? (Sx2 Lam + Lam Sx2)/2 : Lam),   Sx2 = S (x) I2,
+ *   H = (Sm2 Hao Sm2 + its conjugate transpose)/2,                 Sm2 = S^-1/2 (x) I2,
+ * into H (2N x 2N complex). evmin receives the smallest eigenvalue of S. Returns 0, 1 if S is
+ * not positive definite (evmin <= 1e-8: the reference stops there) or its eigenproblem did not
+ * converge, -1 for bad arguments, or a CUDA error (< 0). 1 <= N <= 2048. */
+int qs_dftb_lowdin(int N, const double *S, const double *H0, const double *Lam, int soc_dual, double *H,
+                   double *evmin, int device);
+
 /* pack_gf / unpack_gf (common/linear_algebra.f90:155-233) for nb x nb x Nw arrays. */
 int qs_pack_gf(int nb, int Nw, const double *Gr, const double *Gl, double *out);
 int qs_unpack_gf(int nb, int Nw, const double *in, double *Gr, double *Gl);

@@ -1,0 +1,600 @@
+// setup.cu -- the dense linear algebra of the model set-up, on the device.
+//
+//   qs_hermitian_eigensystem  hermitian_eigensystem (common/linear_algebra.f90:32-56, LAPACK
+//                             zheev) over a batch of matrices of one size; the program calls
+//                             it for the energy grid (src/quichotte.f90:79-83).
+//   qs_dftb_lowdin            the dense part of build_hamiltonian_from_dftb_hs
+//                             (src/hamiltonian.f90:625-640, 680-689): S^-1/2 from the
+//                             eigenpairs of S (dsyev there), the SOC form on the spin-doubled
+//                             basis and H = S^-1/2 Hao S^-1/2, made Hermitian.
+//
+// Eigenproblem: two-sided cyclic Jacobi in the round-robin (tournament) pair order, so the
+// M/2 rotations of one round (M = N rounded up to even) act on disjoint index pairs and run
+// at once. A round is two kernels:
+//   jac_params   one thread per pair: the rotation that zeroes A(p,q), written as a pair
+//                record and as two row records (the coefficients row p and row q take);
+//   jac_rotate   each group of threads owns the two columns of one pair: it rotates them
+//                (A J, and Z J for the eigenvectors), stages A J's two columns in shared
+//                memory and applies the row rotations of all pairs to them (J^H A J).
+// Every access is down a column, so A and Z stay column-major and coalesced. The M-1 rounds
+// of a sweep and the convergence test are one CUDA graph, replayed once per sweep; the host
+// reads one counter per sweep. A matrix is converged when its off-diagonal weight is at
+// rounding level, sum_{i!=j} |a_ij|^2 <= (N eps)^2 sum |a_ij|^2; then every eigenvalue is
+// within about N eps ||A||_F of the exact one, the accuracy class of zheev.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "qs_common.cuh"
+
+namespace qs {
+namespace {
+
+constexpr int JAC_MAX_N = 2048;
+constexpr int JAC_MAX_SWEEPS = 60;
+constexpr int JAC_THREADS = 256;
+
+struct __align__(16) JacPair {
+    double c, s, phx, phy;  // rotation: c, s and the phase of A(p,q)
+    double app, aqq;        // the pivot block's diagonal after the rotation
+    int p, q;               // p < q; q >= N marks the idle slot of an odd N
+};
+struct __align__(16) JacRow {
+    double c, bx, by;  // A''(j,k) = c A'(j,k) + (bx + i by) A'(partner,k)
+    int partner;
+};
+
+// index pair of slot i in round r of the round-robin order over M (even) indices
+__device__ __forceinline__ void jac_slot(int M, int r, int i, int &p, int &q) {
+    if (i == 0) {
+        p = r;
+        q = M - 1;
+    } else {
+        p = (r + i) % (M - 1);
+        q = (r - i + (M - 1)) % (M - 1);
+    }
+    if (p > q) {
+        int t = p;
+        p = q;
+        q = t;
+    }
+}
+
+__global__ void jac_init(int N, int64_t total, zc *__restrict__ A, zc *__restrict__ Z) {
+    const int64_t nn = (int64_t)N * N;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t % nn;
+        const int i = (int)(e % N), j = (int)(e / N);
+        Z[t] = zc{i == j ? 1.0 : 0.0, 0.0};
+        if (i == j) A[t].y = 0.0;  // the diagonal of a Hermitian matrix is real
+    }
+}
+
+// done[b]: 0 active, 1 converged, 2 not finite (stops; reported as not converged).
+// One block per matrix; counts the active matrices into *active.
+__global__ void jac_check(int N, const zc *__restrict__ A, int *__restrict__ done, int *__restrict__ active) {
+    const int b = blockIdx.x;
+    if (done[b]) return;
+    const zc *a = A + (int64_t)b * N * N;
+    double off = 0.0, tot = 0.0;
+    for (int64_t e = threadIdx.x; e < (int64_t)N * N; e += blockDim.x) {
+        const zc v = a[e];
+        const double w = v.x * v.x + v.y * v.y;
+        tot += w;
+        if (e % N != e / N) off += w;
+    }
+    __shared__ double so[32], st[32];
+    for (int o = 16; o; o >>= 1) {
+        off += __shfl_xor_sync(0xffffffffu, off, o);
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        so[threadIdx.x >> 5] = off;
+        st[threadIdx.x >> 5] = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        off = 0.0;
+        tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            off += so[w];
+            tot += st[w];
+        }
+        const double ne = (double)N * 2.220446049250313e-16;
+        int d = 0;
+        if (!(off < INFINITY) || !(tot < INFINITY)) d = 2;  // NaN or Inf entries
+        else if (off <= ne * ne * tot) d = 1;
+        done[b] = d;
+        if (d == 0) atomicAdd(active, 1);
+    }
+}
+
+__global__ void jac_params(int N, int M, int r, int batch, const zc *__restrict__ A, const int *__restrict__ done,
+                           JacPair *__restrict__ pairs, JacRow *__restrict__ rows) {
+    const int S = M / 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= S * batch) return;
+    const int b = t / S, i = t - b * S;
+    if (done[b]) return;
+    int p, q;
+    jac_slot(M, r, i, p, q);
+    const zc *a = A + (int64_t)b * N * N;
+    JacPair P;
+    P.p = p;
+    P.q = q;
+    P.c = 1.0;
+    P.s = 0.0;
+    P.phx = 1.0;
+    P.phy = 0.0;
+    JacRow *R = rows + (int64_t)b * M;
+    if (q >= N) {  // p has no partner this round
+        P.app = a[p + (int64_t)p * N].x;
+        P.aqq = 0.0;
+        pairs[t] = P;
+        R[p] = JacRow{1.0, 0.0, 0.0, p};
+        return;
+    }
+    const double app = a[p + (int64_t)p * N].x, aqq = a[q + (int64_t)q * N].x;
+    const zc apq = a[p + (int64_t)q * N];
+    const double mag = hypot(apq.x, apq.y);
+    P.app = app;
+    P.aqq = aqq;
+    if (mag > 0.0) {
+        // R = [[c, s], [-s, c]] diagonalises [[app, mag], [mag, aqq]]: t = tan(theta) is the
+        // smaller root of t^2 + 2 tau t - 1 = 0, tau = (aqq - app) / (2 mag)
+        const double tau = (aqq - app) / (2.0 * mag);
+        const double tt = fabs(tau) > 1e150 ? 0.5 / tau : copysign(1.0, tau) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = 1.0 / sqrt(1.0 + tt * tt);
+        P.c = c;
+        P.s = tt * c;
+        P.phx = apq.x / mag;
+        P.phy = apq.y / mag;
+        P.app = app - tt * mag;
+        P.aqq = aqq + tt * mag;
+    }
+    pairs[t] = P;
+    // J = [[c, s ph], [-s conj(ph), c]] on (p, q);  J^H rows: p <- c p - s ph q, q <- c q + s conj(ph) p
+    R[p] = JacRow{P.c, -P.s * P.phx, -P.s * P.phy, q};
+    R[q] = JacRow{P.c, P.s * P.phx, -P.s * P.phy, p};
+}
+
+// grid (ceil(S / groups), batch), JAC_THREADS threads in groups of G; shared: groups x 2N complex
+__global__ void __launch_bounds__(JAC_THREADS) jac_rotate(int N, int M, int G, zc *__restrict__ A, zc *__restrict__ Z,
+                                                           const int *__restrict__ done,
+                                                           const JacPair *__restrict__ pairs,
+                                                           const JacRow *__restrict__ rows) {
+    extern __shared__ zc jsm[];
+    const int S = M / 2, groups = JAC_THREADS / G;
+    const int b = blockIdx.y;
+    if (done[b]) return;
+    const int gi = threadIdx.x / G, lt = threadIdx.x - gi * G;
+    const int slot = blockIdx.x * groups + gi;
+    const bool have = slot < S;
+    zc *a = A + (int64_t)b * N * N, *z = Z + (int64_t)b * N * N;
+    zc *cp = jsm + (int64_t)gi * 2 * N, *cq = cp + N;
+    JacPair P{};
+    if (have) P = pairs[(int64_t)b * S + slot];
+    const bool two = have && P.q < N;
+    // A J and Z J on columns p, q:  p' = c p - s conj(ph) q,  q' = c q + s ph p
+    const zc wp = zc{-P.s * P.phx, P.s * P.phy}, wq = zc{P.s * P.phx, P.s * P.phy};
+    if (have) {
+        zc *ap = a + (int64_t)P.p * N, *aq = a + (int64_t)P.q * N;
+        zc *zp = z + (int64_t)P.p * N, *zq = z + (int64_t)P.q * N;
+        for (int j = lt; j < N; j += G) {
+            if (two) {
+                const zc x = ap[j], y = aq[j];
+                zc u = P.c * x, v = P.c * y;
+                cfma(u, wp, y);
+                cfma(v, wq, x);
+                cp[j] = u;
+                cq[j] = v;
+                const zc zx = zp[j], zy = zq[j];
+                zc zu = P.c * zx, zv = P.c * zy;
+                cfma(zu, wp, zy);
+                cfma(zv, wq, zx);
+                zp[j] = zu;
+                zq[j] = zv;
+            } else {
+                cp[j] = ap[j];
+            }
+        }
+    }
+    __syncthreads();
+    if (!have) return;
+    // J^H (A J) on the staged columns, every row j with its own pair's coefficients
+    const JacRow *R = rows + (int64_t)b * M;
+    zc *ap = a + (int64_t)P.p * N, *aq = a + (int64_t)P.q * N;
+    for (int j = lt; j < N; j += G) {
+        const JacRow w = R[j];
+        const zc bw = zc{w.bx, w.by};
+        zc u = w.c * cp[j];
+        cfma(u, bw, cp[w.partner]);
+        if (j == P.p) u = zc{P.app, 0.0};
+        else if (two && j == P.q) u = zc{0.0, 0.0};
+        ap[j] = u;
+        if (two) {
+            zc v = w.c * cq[j];
+            cfma(v, bw, cq[w.partner]);
+            if (j == P.q) v = zc{P.aqq, 0.0};
+            else if (j == P.p) v = zc{0.0, 0.0};
+            aq[j] = v;
+        }
+    }
+}
+
+// eigenvalues ascending (ties and non-finite values in index order, NaN last) and the rank of
+// every diagonal entry; one block per matrix
+__global__ void jac_sort(int N, const zc *__restrict__ A, double *__restrict__ E, int *__restrict__ rank) {
+    extern __shared__ double dk[];
+    const int b = blockIdx.x;
+    const zc *a = A + (int64_t)b * N * N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const double d = a[i + (int64_t)i * N].x;
+        dk[i] = d;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const double di = dk[i];
+        const double ki = isnan(di) ? INFINITY : di;
+        const bool ni = isnan(di);
+        int k = 0;
+        for (int j = 0; j < N; j++) {
+            const double dj = dk[j];
+            const bool nj = isnan(dj);
+            const double kj = nj ? INFINITY : dj;
+            // order: (key, NaN after finite/inf, index)
+            const bool before = kj < ki || (kj == ki && (nj < ni || (nj == ni && j < i)));
+            k += before;
+        }
+        rank[(int64_t)b * N + i] = k;
+        E[(int64_t)b * N + k] = di;
+    }
+}
+
+__global__ void jac_permute(int N, int64_t total, const zc *__restrict__ Z, const int *__restrict__ rank,
+                            zc *__restrict__ V) {
+    const int64_t nn = (int64_t)N * N;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / nn, e = t - b * nn;
+        const int i = (int)(e % N), j = (int)(e / N);
+        V[b * nn + i + (int64_t)rank[b * N + j] * N] = Z[t];
+    }
+}
+
+int grid_for(int64_t total) { return (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 16)); }
+
+// Jacobi on `batch` matrices of order N in dA (device, overwritten: eigenvectors in the
+// columns, ascending), eigenvalues into dE. dinfo[b] = 0, or 1 for a matrix that did not
+// converge (or held non-finite entries). dW: N*N*batch complex workspace (the rotated
+// eigenvectors). Runs on `st`; returns a CUDA error code.
+cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int *dinfo, zc *dW) {
+    const int M = N + (N & 1), S = M / 2;
+    const int64_t total = (int64_t)N * N * batch;
+    int *dflag = nullptr, *dact = nullptr, *drank = nullptr;
+    JacPair *dpairs = nullptr;
+    JacRow *drows = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e;
+    int G = 32;
+    while (G < N && G < JAC_THREADS) G *= 2;
+    const int groups = JAC_THREADS / G;
+    const size_t smem = sizeof(zc) * 2 * (size_t)N * groups;
+    const dim3 rgrid((S + groups - 1) / groups, batch);
+    const int pgrid = (S * batch + 127) / 128;
+    int active = 0, sweeps = 0;
+    std::vector<int> hflag(batch);
+#define JAC_TRY(x)                          \
+    do {                                    \
+        if ((e = (x)) != cudaSuccess) goto out; \
+    } while (0)
+    JAC_TRY(cudaMallocAsync(&dflag, sizeof(int) * (batch + 1), st));
+    dact = dflag + batch;
+    JAC_TRY(cudaMallocAsync(&drank, sizeof(int) * (size_t)N * batch, st));
+    JAC_TRY(cudaMallocAsync(&dpairs, sizeof(JacPair) * (size_t)S * batch, st));
+    JAC_TRY(cudaMallocAsync(&drows, sizeof(JacRow) * (size_t)M * batch, st));
+    JAC_TRY(smem_cap((const void *)jac_rotate));
+    JAC_TRY(smem_cap((const void *)jac_sort));
+    JAC_TRY(cudaMemsetAsync(dflag, 0, sizeof(int) * (batch + 1), st));
+    jac_init<<<grid_for(total), 256, 0, st>>>(N, total, dA, dW);
+    count_launch();
+    jac_check<<<batch, 256, 0, st>>>(N, dA, dflag, dact);
+    count_launch();
+    JAC_TRY(cudaGetLastError());
+    JAC_TRY(cudaMemcpyAsync(&active, dact, sizeof(int), cudaMemcpyDeviceToHost, st));
+    JAC_TRY(cudaStreamSynchronize(st));
+    if (active > 0) {
+        // one sweep: M-1 rounds, then the convergence test of every matrix still active
+        JAC_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < M - 1; r++) {
+            jac_params<<<pgrid, 128, 0, st>>>(N, M, r, batch, dA, dflag, dpairs, drows);
+            jac_rotate<<<rgrid, JAC_THREADS, smem, st>>>(N, M, G, dA, dW, dflag, dpairs, drows);
+        }
+        cudaMemsetAsync(dact, 0, sizeof(int), st);
+        jac_check<<<batch, 256, 0, st>>>(N, dA, dflag, dact);
+        e = cudaStreamEndCapture(st, &graph);
+        if (e != cudaSuccess) goto out;
+        JAC_TRY(cudaGraphInstantiate(&exec, graph, 0));
+        while (active > 0 && sweeps < JAC_MAX_SWEEPS) {
+            JAC_TRY(cudaGraphLaunch(exec, st));
+            for (int k = 0; k < 2 * (M - 1) + 1; k++) count_launch();
+            JAC_TRY(cudaMemcpyAsync(&active, dact, sizeof(int), cudaMemcpyDeviceToHost, st));
+            JAC_TRY(cudaStreamSynchronize(st));
+            sweeps++;
+        }
+    }
+    jac_sort<<<batch, 256, sizeof(double) * N, st>>>(N, dA, dE, drank);
+    count_launch();
+    jac_permute<<<grid_for(total), 256, 0, st>>>(N, total, dW, drank, dA);
+    count_launch();
+    JAC_TRY(cudaGetLastError());
+    JAC_TRY(cudaMemcpyAsync(hflag.data(), dflag, sizeof(int) * batch, cudaMemcpyDeviceToHost, st));
+    JAC_TRY(cudaStreamSynchronize(st));
+    for (int b = 0; b < batch; b++) hflag[b] = hflag[b] == 1 ? 0 : 1;
+    JAC_TRY(cudaMemcpyAsync(dinfo, hflag.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, st));
+    JAC_TRY(cudaStreamSynchronize(st));
+out:
+#undef JAC_TRY
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaStreamCaptureStatus cs;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+    }
+    if (dflag) cudaFreeAsync(dflag, st);
+    if (drank) cudaFreeAsync(drank, st);
+    if (dpairs) cudaFreeAsync(dpairs, st);
+    if (drows) cudaFreeAsync(drows, st);
+    cudaStreamSynchronize(st);
+    return e;
+}
+
+// ---- Loewdin transform ----
+
+// C = alpha A op(B) + beta C, complex FP64, column-major, op(B) = B or B^H; 64x64 tiles of C,
+// 256 threads with a 4x4 block each (the set-up's few products; not on the SCF path)
+constexpr int GT = 64, GK = 8;
+__global__ void __launch_bounds__(256) zgemm_small(int m, int n, int k, const zc *__restrict__ A, int lda,
+                                                  const zc *__restrict__ B, int ldb, bool conjB, zc *__restrict__ C,
+                                                  int ldc, double alpha, double beta) {
+    __shared__ zc As[GK][GT + 1], Bs[GK][GT + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int i0 = blockIdx.x * GT, j0 = blockIdx.y * GT;
+    zc acc[4][4] = {};
+    for (int k0 = 0; k0 < k; k0 += GK) {
+        for (int e = threadIdx.x; e < GK * GT; e += 256) {
+            {  // A(i0 + ii, k0 + kk): ii fastest, down a column
+                const int kk = e / GT, ii = e % GT, gi = i0 + ii, gk = k0 + kk;
+                As[kk][ii] = (gi < m && gk < k) ? A[gi + (int64_t)gk * lda] : zc{0.0, 0.0};
+            }
+            if (conjB) {  // B^H(k, j) = conj(B(j, k)): j fastest
+                const int kk = e / GT, jj = e % GT, gj = j0 + jj, gk = k0 + kk;
+                Bs[kk][jj] = (gj < n && gk < k) ? conj(B[gj + (int64_t)gk * ldb]) : zc{0.0, 0.0};
+            } else {      // B(k, j): k fastest
+                const int kk = e % GK, jj = e / GK, gj = j0 + jj, gk = k0 + kk;
+                Bs[kk][jj] = (gj < n && gk < k) ? B[gk + (int64_t)gj * ldb] : zc{0.0, 0.0};
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GK; kk++) {
+            zc av[4], bv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                av[u] = As[kk][tx + 16 * u];
+                bv[u] = Bs[kk][ty + 16 * u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) cfma(acc[u][v], av[u], bv[v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const int gi = i0 + tx + 16 * u, gj = j0 + ty + 16 * v;
+            if (gi < m && gj < n) {
+                zc *c = C + gi + (int64_t)gj * ldc;
+                const zc old = beta == 0.0 ? zc{0.0, 0.0} : beta * *c;
+                *c = old + alpha * acc[u][v];
+            }
+        }
+}
+
+void zgemm(cudaStream_t st, int m, int n, int k, const zc *A, int lda, const zc *B, int ldb, bool conjB, zc *C,
+           int ldc, double alpha, double beta) {
+    dim3 grid((m + GT - 1) / GT, (n + GT - 1) / GT);
+    zgemm_small<<<grid, 256, 0, st>>>(m, n, k, A, lda, B, ldb, conjB, C, ldc, alpha, beta);
+    count_launch();
+}
+
+// W(:,k) = Z(:,k) / ev_k^(1/4) (src/hamiltonian.f90:636-639), and the minimum eigenvalue
+__global__ void lowdin_scale(int N, const double *__restrict__ ev, zc *__restrict__ Z) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N * N; t += gridDim.x * blockDim.x) {
+        const int k = t / N;
+        const double f = 1.0 / sqrt(sqrt(ev[k]));
+        Z[t] = f * Z[t];
+    }
+}
+
+// X2(2i+s, 2j+s) = X(i,j) (spin doubling, spin fastest; src/hamiltonian.f90:672-680)
+__global__ void spin_double(int N, const zc *__restrict__ X, zc *__restrict__ X2) {
+    const int No = 2 * N;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < No * No; t += gridDim.x * blockDim.x) {
+        const int r = t % No, c = t / No;
+        X2[t] = (r & 1) == (c & 1) ? X[(r >> 1) + (int64_t)(c >> 1) * N] : zc{0.0, 0.0};
+    }
+}
+
+// y += a x
+__global__ void zaxpy_k(int64_t n, double a, const zc *__restrict__ x, zc *__restrict__ y) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        y[t] = y[t] + a * x[t];
+}
+
+__global__ void real_to_complex(int64_t n, const double *__restrict__ x, zc *__restrict__ z) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        z[t] = zc{x[t], 0.0};
+}
+
+// H = (Hn + Hn^H) / 2 (src/hamiltonian.f90:689)
+__global__ void hermitize(int n, const zc *__restrict__ Hn, zc *__restrict__ H) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * n; t += gridDim.x * blockDim.x) {
+        const int i = t % n, j = t / n;
+        H[t] = 0.5 * (Hn[t] + conj(Hn[j + (int64_t)i * n]));
+    }
+}
+
+// makes `device` current for the scope of a call (device < 0: leaves the current one)
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int device) {
+        if (device < 0) return;
+        if ((err = cudaGetDevice(&prev)) == cudaSuccess) err = cudaSetDevice(device);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+}  // namespace qs
+
+using namespace qs;
+
+extern "C" {
+
+int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, int device) {
+    if (N < 1 || N > JAC_MAX_N || batch < 0 || batch > 65535 || (batch > 0 && (!A || !E))) return -1;
+    if (batch == 0) return 0;
+    DeviceScope ds(device);
+    if (ds.err != cudaSuccess) return -(int)ds.err;
+    const size_t nn = (size_t)N * N * batch;
+    cudaStream_t st = nullptr;
+    zc *dA = nullptr, *dW = nullptr;
+    double *dE = nullptr;
+    int *dinfo = nullptr;
+    std::vector<int> hinfo(batch, 0);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return -(int)e;
+    if ((e = cudaMallocAsync(&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (e = cudaMallocAsync(&dW, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (e = cudaMallocAsync(&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
+        (e = cudaMallocAsync(&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess &&
+        (e = eigh_dev(st, N, batch, dA, dE, dinfo, dW)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(A, dA, sizeof(zc) * nn, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(E, dE, sizeof(double) * (size_t)N * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (dA) cudaFreeAsync(dA, st);
+    if (dW) cudaFreeAsync(dW, st);
+    if (dE) cudaFreeAsync(dE, st);
+    if (dinfo) cudaFreeAsync(dinfo, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return -(int)e;
+    int bad = 0;
+    for (int b = 0; b < batch; b++) {
+        if (info) info[b] = hinfo[b];
+        bad |= hinfo[b];
+    }
+    return bad ? 1 : 0;
+}
+
+int qs_dftb_lowdin(int N, const double *S, const double *H0, const double *Lam, int soc_dual, double *H,
+                   double *evmin, int device) {
+    if (N < 1 || N > JAC_MAX_N || !S || !H0 || !Lam || !H) return -1;
+    DeviceScope ds(device);
+    if (ds.err != cudaSuccess) return -(int)ds.err;
+    const int No = 2 * N;
+    const size_t n1 = (size_t)N * N, n2 = (size_t)No * No;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return -(int)e;
+    zc *buf = nullptr;
+    double *dR = nullptr;
+    int *dinfo = nullptr;
+    int rc = 0, hinfo = 0;
+    std::vector<double> ev(N);
+    const int gb = 148 * 8;
+#define LOW_TRY(x)                          \
+    do {                                    \
+        if ((e = (x)) != cudaSuccess) goto out; \
+    } while (0)
+    // n1 blocks: S then its eigenvectors, the eigensolver's workspace, S^-1/2;
+    // n2 blocks: Sm2, Lam, Hao, T, Hn.  dR: S, H0 (real), the eigenvalues of S
+    LOW_TRY(cudaMallocAsync(&buf, sizeof(zc) * (3 * n1 + 5 * n2), st));
+    LOW_TRY(cudaMallocAsync(&dR, sizeof(double) * (2 * n1 + N), st));
+    LOW_TRY(cudaMallocAsync(&dinfo, sizeof(int), st));
+    {
+        zc *dS = buf, *dW = buf + n1, *dSmh = buf + 2 * n1;
+        zc *dSm2 = buf + 3 * n1, *dLam = dSm2 + n2, *dHao = dLam + n2, *dT = dHao + n2, *dHn = dT + n2;
+        double *dE = dR + 2 * n1;
+        LOW_TRY(cudaMemcpyAsync(dR, S, sizeof(double) * n1, cudaMemcpyHostToDevice, st));
+        LOW_TRY(cudaMemcpyAsync(dR + n1, H0, sizeof(double) * n1, cudaMemcpyHostToDevice, st));
+        LOW_TRY(cudaMemcpyAsync(dLam, Lam, sizeof(zc) * n2, cudaMemcpyHostToDevice, st));
+        // S^-1/2 = U diag(ev^-1/2) U^T (src/hamiltonian.f90:627-640)
+        real_to_complex<<<gb, 256, 0, st>>>((int64_t)n1, dR, dS);
+        count_launch();
+        LOW_TRY(eigh_dev(st, N, 1, dS, dE, dinfo, dW));
+        LOW_TRY(cudaMemcpyAsync(ev.data(), dE, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+        LOW_TRY(cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+        LOW_TRY(cudaStreamSynchronize(st));
+        double mn = ev[0];
+        for (int k = 1; k < N; k++) mn = std::fmin(mn, ev[k]);
+        if (evmin) *evmin = mn;
+        if (hinfo || !(mn > 1e-8)) {  // eigensolver failure or S not positive definite: the reference stops
+            rc = 1;
+            goto out;
+        }
+        lowdin_scale<<<gb, 256, 0, st>>>(N, dE, dS);
+        count_launch();
+        zgemm(st, N, N, N, dS, N, dS, N, true, dSmh, N, 1.0, 0.0);  // W W^T, W real
+        spin_double<<<gb, 256, 0, st>>>(N, dSmh, dSm2);
+        count_launch();
+        // Hao = H0 spin-doubled, plus the SOC form (src/hamiltonian.f90:670-687)
+        real_to_complex<<<gb, 256, 0, st>>>((int64_t)n1, dR + n1, dW);
+        count_launch();
+        spin_double<<<gb, 256, 0, st>>>(N, dW, dHao);
+        count_launch();
+        if (soc_dual) {
+            real_to_complex<<<gb, 256, 0, st>>>((int64_t)n1, dR, dW);
+            count_launch();
+            spin_double<<<gb, 256, 0, st>>>(N, dW, dT);  // Sx2
+            count_launch();
+            zgemm(st, No, No, No, dT, No, dLam, No, false, dHao, No, 0.5, 1.0);
+            zgemm(st, No, No, No, dLam, No, dT, No, false, dHao, No, 0.5, 1.0);
+        } else {
+            zaxpy_k<<<gb, 256, 0, st>>>((int64_t)n2, 1.0, dLam, dHao);
+            count_launch();
+        }
+        // H = Sm2 (Hao Sm2), then (H + H^H) / 2 (src/hamiltonian.f90:688-689)
+        zgemm(st, No, No, No, dHao, No, dSm2, No, false, dT, No, 1.0, 0.0);
+        zgemm(st, No, No, No, dSm2, No, dT, No, false, dHn, No, 1.0, 0.0);
+        hermitize<<<gb, 256, 0, st>>>(No, dHn, dHao);
+        count_launch();
+        LOW_TRY(cudaGetLastError());
+        LOW_TRY(cudaMemcpyAsync(H, dHao, sizeof(zc) * n2, cudaMemcpyDeviceToHost, st));
+        LOW_TRY(cudaStreamSynchronize(st));
+    }
+out:
+#undef LOW_TRY
+    if (buf) cudaFreeAsync(buf, st);
+    if (dR) cudaFreeAsync(dR, st);
+    if (dinfo) cudaFreeAsync(dinfo, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return -(int)e;
+    return rc;
+}
+
+}  // extern "C"

@@ -255,6 +255,8 @@ void jacobi_herm(int n, std::vector<cplx> A, std::vector<double> &E, std::vector
 struct Model {
     std::string dir;
     FILE *log = nullptr;
+    const qsh_solver_api *api = nullptr;  // its set-up linear algebra, where it has some
+    int device = 0;
     // Parameters
     int N_sites = 0, Norb = 0, n_omega = 0, n_volt_steps = 0, N_ions = 0, N_turns = 0, order = 0;
     std::string hamiltonian_model = "helix", xyz_file = "molecule.xyz",
@@ -938,35 +940,24 @@ struct Model {
         }
     }
 
-    // src/hamiltonian.f90:606-708
-    void build_from_dftb_hs() {
-        const double hartree = 27.211386245988;
-        int N = N_sites;
-        std::vector<double> S, H0;
-        read_dftb_square(overlap_file, N, S);
-        read_dftb_square(ham_file, N, H0);
-        std::vector<double> Ss((size_t)N * N), Hs((size_t)N * N);
-        for (int j = 0; j < N; j++)
-            for (int i = 0; i < N; i++) {
-                Ss[i + (size_t)j * N] = 0.5 * (S[i + (size_t)j * N] + S[j + (size_t)i * N]);
-                Hs[i + (size_t)j * N] = 0.5 * (H0[i + (size_t)j * N] + H0[j + (size_t)i * N]) * hartree;
-            }
-        // S^-1/2 = U diag(1/sqrt(s)) U^T
-        std::vector<cplx> Sc(Ss.begin(), Ss.end()), Z;
-        std::vector<double> ev;
-        jacobi_herm(N, Sc, ev, Z);
-        double evmin = *std::min_element(ev.begin(), ev.end());
-        if (evmin <= 1e-8) fail(" ERROR: overlap matrix is not positive definite (min eigenvalue " + std::to_string(evmin) + ")");
-        std::vector<double> U((size_t)N * N), Smh((size_t)N * N, 0.0);
-        for (int k = 0; k < N; k++)
-            for (int i = 0; i < N; i++) U[i + (size_t)k * N] = Z[i + (size_t)k * N].real() / std::sqrt(std::sqrt(ev[k]));
-        for (int j = 0; j < N; j++)
-            for (int i = 0; i < N; i++) {
-                double s = 0;
-                for (int k = 0; k < N; k++) s += U[i + (size_t)k * N] * U[j + (size_t)k * N];
-                Smh[i + (size_t)j * N] = s;
-            }
+    // the dense part on the solver's device (qs_dftb_lowdin): S^-1/2, the SOC form, H
+    // (src/hamiltonian.f90:625-689); Lam as below (src/hamiltonian.f90:645-668)
+    void build_dftb_lowdin_device(int N, const std::vector<double> &Ss, const std::vector<double> &Hs) {
+        std::vector<cplx> Lam = soc_matrix();
+        std::vector<cplx> Hn((size_t)Norb * Norb);
+        double evmin = 0.0;
+        int rc = api->dftb_lowdin(N, Ss.data(), Hs.data(), (const double *)Lam.data(), soc_form == "dual" ? 1 : 0,
+                                  (double *)Hn.data(), &evmin, device);
+        if (rc == 1) fail(" ERROR: overlap matrix is not positive definite (min eigenvalue " + std::to_string(evmin) + ")");
+        if (rc != 0) fail(" ERROR: device set-up failed (dftb_lowdin status " + std::to_string(rc) + ")");
         say(" DFTB H0/S: smallest overlap eigenvalue = %10.2E\n", evmin);
+        if (soc_form != "dual" && soc_form != "onsite") fail(" ERROR: soc_form must be dual or onsite, not " + soc_form);
+        H = Hn;
+        say(" DFTB H0/S Hamiltonian: %d atoms, %d orbitals, SOC form %s\n", N_atoms, N, soc_form.c_str());
+    }
+
+    // (L.S) xi on the p shells in the AO basis, spin fastest (src/hamiltonian.f90:645-668)
+    std::vector<cplx> soc_matrix() const {
         // (L_k)_ab = -i eps_kab ; Pauli matrices
         cplx Lk[3][3][3] = {};
         Lk[0][1][2] = -IM; Lk[0][2][1] = IM;
@@ -994,6 +985,43 @@ struct Model {
                                     xi * Lk[k][pidx[p - 1]][pidx[q - 1]] * sig[s1 - 1][s2 - 1][k] / 2.0;
                         }
         }
+        return Lam;
+    }
+
+    // src/hamiltonian.f90:606-708
+    void build_from_dftb_hs() {
+        const double hartree = 27.211386245988;
+        int N = N_sites;
+        std::vector<double> S, H0;
+        read_dftb_square(overlap_file, N, S);
+        read_dftb_square(ham_file, N, H0);
+        std::vector<double> Ss((size_t)N * N), Hs((size_t)N * N);
+        for (int j = 0; j < N; j++)
+            for (int i = 0; i < N; i++) {
+                Ss[i + (size_t)j * N] = 0.5 * (S[i + (size_t)j * N] + S[j + (size_t)i * N]);
+                Hs[i + (size_t)j * N] = 0.5 * (H0[i + (size_t)j * N] + H0[j + (size_t)i * N]) * hartree;
+            }
+        if (api && api->dftb_lowdin) {
+            build_dftb_lowdin_device(N, Ss, Hs);
+            return;
+        }
+        // S^-1/2 = U diag(1/sqrt(s)) U^T
+        std::vector<cplx> Sc(Ss.begin(), Ss.end()), Z;
+        std::vector<double> ev;
+        jacobi_herm(N, Sc, ev, Z);
+        double evmin = *std::min_element(ev.begin(), ev.end());
+        if (evmin <= 1e-8) fail(" ERROR: overlap matrix is not positive definite (min eigenvalue " + std::to_string(evmin) + ")");
+        std::vector<double> U((size_t)N * N), Smh((size_t)N * N, 0.0);
+        for (int k = 0; k < N; k++)
+            for (int i = 0; i < N; i++) U[i + (size_t)k * N] = Z[i + (size_t)k * N].real() / std::sqrt(std::sqrt(ev[k]));
+        for (int j = 0; j < N; j++)
+            for (int i = 0; i < N; i++) {
+                double s = 0;
+                for (int k = 0; k < N; k++) s += U[i + (size_t)k * N] * U[j + (size_t)k * N];
+                Smh[i + (size_t)j * N] = s;
+            }
+        say(" DFTB H0/S: smallest overlap eigenvalue = %10.2E\n", evmin);
+        std::vector<cplx> Lam = soc_matrix();
         std::vector<cplx> Sx2((size_t)Norb * Norb, 0.0), Sm2((size_t)Norb * Norb, 0.0), Hao((size_t)Norb * Norb, 0.0);
         for (int j = 1; j <= N; j++)
             for (int i = 1; i <= N; i++)
@@ -1045,8 +1073,17 @@ struct Model {
 
     // src/quichotte.f90:241-253 energy grid from the spectrum of H
     void energy_grid() {
-        std::vector<cplx> Z;
-        jacobi_herm(Norb, H, Ev, Z);
+        if (api && api->hermitian_eigensystem) {
+            std::vector<cplx> A = H;
+            Ev.assign(Norb, 0.0);
+            int info = 0;
+            int rc = api->hermitian_eigensystem(Norb, 1, (double *)A.data(), Ev.data(), &info, device);
+            if (rc == 1) fail(" ERROR: ZHEEV eigenproblem failed, INFO = " + std::to_string(info));
+            if (rc != 0) fail(" ERROR: device set-up failed (hermitian_eigensystem status " + std::to_string(rc) + ")");
+        } else {
+            std::vector<cplx> Z;
+            jacobi_herm(Norb, H, Ev, Z);
+        }
         w_init = Ev.front() - dw;
         w_fin = Ev.back() + up;
         n_omega = (int)((w_fin - w_init) / delta);  // Fortran int(): truncation
@@ -1137,9 +1174,16 @@ int fmt_real(double x, char *buf) {
 extern "C" {
 
 int qsh_load(const char *dir, qsh_model **out, char *errbuf, int errlen, FILE *log) {
+    return qsh_load_with(dir, nullptr, 0, out, errbuf, errlen, log);
+}
+
+int qsh_load_with(const char *dir, const qsh_solver_api *api, int device, qsh_model **out, char *errbuf, int errlen,
+                  FILE *log) {
     Model m;
     m.dir = dir ? dir : ".";
     m.log = log;
+    m.api = api;
+    m.device = device;
     try {
         m.read_input();
         m.build_hamiltonian();

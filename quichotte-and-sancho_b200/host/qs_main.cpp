@@ -21,7 +21,7 @@ extern "C" int qsh_run(const char *dir, const qsh_solver_api *api, int precision
     auto P = [&](const char *f) { return d + "/" + f; };
     char err[4096] = {0};
     qsh_model *m = nullptr;
-    if (qsh_load(d.c_str(), &m, err, sizeof err, log) != 0) {
+    if (qsh_load_with(d.c_str(), api, device, &m, err, sizeof err, log) != 0) {
         std::fprintf(stderr, "%s\n", err);
         return 1;
     }

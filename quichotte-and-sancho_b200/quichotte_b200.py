@@ -144,7 +144,8 @@ C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current
          "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
          "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
          "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
-         "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice")
+         "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice",
+         "qs_hermitian_eigensystem", "qs_dftb_lowdin")
 TUNE_DYSON, TUNE_KELDYSH, TUNE_SIG2_A, TUNE_SIG2_C = 0, 1, 2, 3
 QS_ERR_NOALLOC_LIMIT = -1001
 QS_ERR_TOO_LARGE = -1002
@@ -195,6 +196,10 @@ _lib.qs_server_destroy.argtypes = [ctypes.c_void_p]
 _lib.qs_server_destroy.restype = None
 _lib.qs_invert_batched_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p]
+_lib.qs_hermitian_eigensystem.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_int]
+_lib.qs_dftb_lowdin.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                ctypes.c_void_p, _dp, ctypes.c_int]
 
 
 def _ptr(a):
@@ -441,6 +446,44 @@ def invert_batched(A, precision=QS_PREC_FP64, lib=None, prefix="qs_"):
     if rc < 0:
         raise SolverError(f"invert_batched failed ({rc})")
     return buf.transpose(0, 2, 1).copy(), info
+
+
+def hermitian_eigensystem(A, device=0):
+    """hermitian_eigensystem (zheev) on the device over a batch. A: (batch, N, N) or (N, N)
+    Hermitian complex. Returns (E ascending, Z with the eigenvectors in its columns, info)
+    with info[b] = 1 for a matrix that did not converge or holds non-finite entries."""
+    A = np.asarray(A, np.complex128)
+    single = A.ndim == 2
+    if single:
+        A = A[None]
+    batch, N, _ = A.shape
+    buf = np.array(A.transpose(0, 2, 1), dtype=np.complex128, order="C", copy=True)
+    E = np.zeros((batch, N))
+    info = np.zeros(batch, np.int32)
+    rc = _lib.qs_hermitian_eigensystem(N, batch, _ptr(buf), _ptr(E), _ptr(info), device)
+    if rc < 0:
+        raise SolverError(f"hermitian_eigensystem failed ({rc})")
+    Z = buf.transpose(0, 2, 1).copy()
+    return (E[0], Z[0], info[0]) if single else (E, Z, info)
+
+
+def dftb_lowdin(S, H0, Lam, soc_dual=True, device=0):
+    """The Loewdin transform of the dftb_hs model on the device: S, H0 (N, N) real, Lam
+    (2N, 2N) complex. Returns (H (2N, 2N) complex, smallest eigenvalue of S); raises for an S
+    that is not positive definite, as the reference stops there."""
+    S = np.asfortranarray(S, np.float64)
+    H0 = np.asfortranarray(H0, np.float64)
+    Lam = np.asfortranarray(Lam, np.complex128)
+    N = S.shape[0]
+    H = np.zeros((2 * N, 2 * N), np.complex128, order="F")
+    evmin = ctypes.c_double(0.0)
+    rc = _lib.qs_dftb_lowdin(N, _ptr(S), _ptr(H0), _ptr(Lam), int(bool(soc_dual)), _ptr(H), ctypes.byref(evmin),
+                             device)
+    if rc == 1:
+        raise SolverError(f"overlap matrix is not positive definite (min eigenvalue {evmin.value:.3e})")
+    if rc != 0:
+        raise SolverError(f"dftb_lowdin failed ({rc})")
+    return H, evmin.value
 
 
 def pack_gf(Gr, Gl, lib=None, prefix="qs_"):
