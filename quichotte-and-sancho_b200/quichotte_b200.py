@@ -92,6 +92,22 @@ RESIDUAL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, _dp, _dp, 
 
 _host.qsh_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(_QshModel)), ctypes.c_char_p, ctypes.c_int,
                            ctypes.c_void_p]
+EIGENSYSTEM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int)
+LOWDIN_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int)
+
+
+class QshSolverApi(ctypes.Structure):
+    """qsh_solver_api of qs_host.h (the solver entry points as plain pointers, then the
+    optional set-up linear algebra)."""
+    _fields_ = ([("name", ctypes.c_char_p)] + [(k, ctypes.c_void_p) for k in ("create", "destroy", "last_error",
+                                                                              "solve_scf", "current",
+                                                                              "get_observables")]
+                + [("hermitian_eigensystem", EIGENSYSTEM_FN), ("dftb_lowdin", LOWDIN_FN)])
+
+
+_host.qsh_load_with.argtypes = [ctypes.c_char_p, ctypes.POINTER(QshSolverApi), ctypes.c_int,
+                                ctypes.POINTER(ctypes.POINTER(_QshModel)), ctypes.c_char_p, ctypes.c_int,
+                                ctypes.c_void_p]
 _host.qsh_helix.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 15 + [ctypes.c_int,
                                                                                      ctypes.POINTER(ctypes.POINTER(_QshModel))]
 _host.qsh_free.argtypes = [ctypes.POINTER(_QshModel)]
@@ -227,6 +243,7 @@ class Model:
         self.GammaR = cp(m.GammaR, 2 * No * No).view(np.complex128).reshape(No, No, order="F")
         self.U_site = cp(m.U_site, No)
         self.omega = cp(m.omega, n)
+        self.Ev = cp(m.Ev, No)
         self.atom_norb = np.ctypeslib.as_array(m.atom_norb, (m.N_atoms,)).astype(np.int32).copy()
         self.atom_first = np.ctypeslib.as_array(m.atom_first, (m.N_atoms,)).astype(np.int32).copy()
         self.model_name = m.model_name.decode()
@@ -241,6 +258,16 @@ class Model:
         p = ctypes.POINTER(_QshModel)()
         err = ctypes.create_string_buffer(4096)
         rc = _host.qsh_load(os.fsencode(case_dir), ctypes.byref(p), err, 4096, None)
+        if rc != 0:
+            raise ValueError(err.value.decode(errors="replace").strip())
+        return cls(p)
+
+    @classmethod
+    def load_with(cls, case_dir, api, device=0):
+        """load with the set-up linear algebra of `api` (a QshSolverApi)."""
+        p = ctypes.POINTER(_QshModel)()
+        err = ctypes.create_string_buffer(4096)
+        rc = _host.qsh_load_with(os.fsencode(case_dir), ctypes.byref(api), device, ctypes.byref(p), err, 4096, None)
         if rc != 0:
             raise ValueError(err.value.decode(errors="replace").strip())
         return cls(p)

@@ -105,3 +105,64 @@ def test_fast_formatter_matches_the_printf_rules():
     for x in vals:
         lib.qsh_fmt_real(x, buf)
         assert buf.value.decode() == _printf_rules(x), repr(x)
+
+
+def _numpy_setup_api(calls, fail_eigensystem=False):
+    """A qsh_solver_api whose set-up linear algebra is LAPACK through numpy (the solver
+    entry points stay NULL: only the model set-up runs)."""
+    def eigensystem(N, batch, A, E, info, device):
+        calls.append("eigensystem")
+        if fail_eigensystem:
+            info[0] = 1
+            return 1
+        a = np.ctypeslib.as_array(A, (batch * N * N * 2,)).view(np.complex128).reshape(batch, N, N)
+        e = np.ctypeslib.as_array(E, (batch * N,)).reshape(batch, N)
+        for b in range(batch):
+            w, v = np.linalg.eigh(a[b].T)  # column-major storage
+            e[b] = w
+            a[b] = v.T
+            info[b] = 0
+        return 0
+
+    def lowdin(N, S, H0, Lam, dual, H, evmin, device):
+        calls.append("lowdin")
+        s = np.ctypeslib.as_array(S, (N * N,)).reshape(N, N).T
+        h0 = np.ctypeslib.as_array(H0, (N * N,)).reshape(N, N).T
+        lam = np.ctypeslib.as_array(Lam, (8 * N * N,)).view(np.complex128).reshape(2 * N, 2 * N).T
+        ev, U = np.linalg.eigh(s)
+        evmin[0] = ev.min()
+        W = U / np.sqrt(np.sqrt(ev))
+        Sx2, Sm2 = np.kron(s, np.eye(2)), np.kron(W @ W.T, np.eye(2))
+        Hao = np.kron(h0, np.eye(2)) + (0.5 * (Sx2 @ lam + lam @ Sx2) if dual else lam)
+        Hn = Sm2 @ Hao @ Sm2
+        out = np.ctypeslib.as_array(H, (8 * N * N,)).view(np.complex128).reshape(2 * N, 2 * N)
+        out[:] = (0.5 * (Hn + Hn.conj().T)).T
+        return 0
+    api = qb.QshSolverApi()
+    api.name = b"numpy-setup"
+    api.hermitian_eigensystem = qb.EIGENSYSTEM_FN(eigensystem)
+    api.dftb_lowdin = qb.LOWDIN_FN(lowdin)
+    api._keep = (api.hermitian_eigensystem, api.dftb_lowdin)
+    return api
+
+
+@pytest.mark.parametrize("case", ["order2_dftb_hs", "order2_second_order"])
+def test_model_setup_through_the_solver_api(case):
+    """qsh_load_with hands the grid eigenproblem and the dftb_hs Loewdin transform to the
+    solver's set-up entry points (the B200 program passes qs_hermitian_eigensystem and
+    qs_dftb_lowdin); with LAPACK behind them the model equals the host-built one."""
+    calls = []
+    api = _numpy_setup_api(calls)
+    m = qb.Model.load_with(os.path.join(CASES, case), api)
+    h = qb.Model.load(os.path.join(CASES, case))
+    assert calls == (["lowdin", "eigensystem"] if case == "order2_dftb_hs" else ["eigensystem"])
+    assert np.max(np.abs(m.H - h.H)) <= 1e-12 * np.max(np.abs(h.H))
+    assert np.max(np.abs(m.Ev - h.Ev)) <= 1e-12 * np.max(np.abs(h.Ev))
+    assert m.n_omega == h.n_omega
+    assert np.max(np.abs(m.omega - h.omega)) <= 1e-12 * np.max(np.abs(h.omega))  # w_init = Ev_min - dw
+
+
+def test_model_setup_failure_is_the_reference_stop():
+    api = _numpy_setup_api([], fail_eigensystem=True)
+    with pytest.raises(ValueError, match="ZHEEV eigenproblem failed"):
+        qb.Model.load_with(os.path.join(CASES, "order2_second_order"), api)
