@@ -127,7 +127,7 @@ __global__ void jac_params(int N, int M, int r, int batch, const zc *__restrict_
     P.phx = 1.0;
     P.phy = 0.0;
     JacRow *R = rows + (int64_t)b * M;
-    if (q >= N) {  // p has no partner this round
+    if (q >= N) {  // p has no partner among these rotations (odd N)
         P.app = a[p + (int64_t)p * N].x;
         P.aqq = 0.0;
         pairs[t] = P;
