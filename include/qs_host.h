@@ -96,9 +96,9 @@ typedef struct qsh_solver_api {
     int (*solve_scf)(void *h, double Volt, int fresh_start, qs_scf_result *res);
     int (*current)(void *h, double Volt, double *J_up, double *J_down);
     int (*get_observables)(void *h, double *G_less_obs, double *dosd, double *trU, double *trD);
-    /* optional: the set-up's dense linear algebra (qs_hermitian_eigensystem, qs_dftb_lowdin
+    /* optional: the set-up's dense linear algebra (qs_hermitian_eigenvalues, qs_dftb_lowdin
      * of qsb200.h); NULL uses the host's own (cyclic Jacobi and plain products) */
-    int (*hermitian_eigensystem)(int N, int batch, double *A, double *E, int *info, int device);
+    int (*hermitian_eigenvalues)(int N, int batch, const double *A, double *E, int *info, int device);
     int (*dftb_lowdin)(int N, const double *S, const double *H0, const double *Lam, int soc_dual, double *H,
                        double *evmin, int device);
 } qsh_solver_api;

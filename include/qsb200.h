@@ -126,6 +126,13 @@ int qs_invert_batched(int N, int batch, double *A, int *info, int precision);
  * 1 if some info[b] != 0, -1 for bad arguments, or a CUDA error (< 0). */
 int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, int device);
 
+/* The same eigenvalues without the eigenvectors (zheev with JOBZ = 'N'), as the energy grid
+ * needs them (src/quichotte.f90:81-83): A is not modified. For N <= 160 each matrix is
+ * diagonalised by one thread block with the matrix in shared memory (one launch for the
+ * batch); larger N takes the path of qs_hermitian_eigensystem. Same info, limits and
+ * returns. */
+int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *info, int device);
+
 /* The dense linear algebra of build_hamiltonian_from_dftb_hs (src/hamiltonian.f90:625-689):
  * S (N x N real symmetric overlap) and H0 (N x N real, eV) as the reference holds them after
  * symmetrisation, Lam (2N x 2N complex, the p-shell SOC matrix, spin fastest);

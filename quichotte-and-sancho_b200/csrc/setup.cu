@@ -353,6 +353,205 @@ out:
     return e;
 }
 
+// ---- eigenvalues only: one block per matrix, the matrix in shared memory ----
+// The upper triangle is packed by columns, (i, j) with i <= j at i + j (j + 1) / 2, so a matrix
+// of order N <= 160 fits one block's shared memory. One rotation round maps every 2x2 block
+// B = A[{p, q}, {p', q'}] of two pairs to J_P^H B J_P' (a pair's own diagonal block becomes
+// diag(app', aqq')); each block is read and written by one thread, so a round needs no second
+// buffer and every sweep runs inside one launch, with block barriers between the phases.
+constexpr int JV_MAX_N = 160, JV_THREADS = 512;
+
+__device__ __forceinline__ int pk(int i, int j) { return i + j * (j + 1) / 2; }  // i <= j
+__device__ __forceinline__ zc pget(const zc *P, int a, int b) { return a <= b ? P[pk(a, b)] : conj(P[pk(b, a)]); }
+__device__ __forceinline__ void pset(zc *P, int a, int b, zc v) {
+    if (a <= b) P[pk(a, b)] = v;
+    else P[pk(b, a)] = conj(v);
+}
+
+constexpr int JV_TASKS = 8;  // 2x2 blocks per thread: S (S + 1) / 2 <= 3240 <= 8 x 512
+
+inline size_t jv_smem(int N) {
+    const size_t M = N + (N & 1), S = M / 2, np = (size_t)N * (N + 1) / 2;
+    return 16 * np + 48 * S + 8 * S + 8 * (size_t)N;
+}
+
+__global__ void __launch_bounds__(JV_THREADS) jac_values(int N, const zc *__restrict__ A, double *__restrict__ E,
+                                                        int *__restrict__ info) {
+    extern __shared__ __align__(16) unsigned char jv_raw[];
+    const int M = N + (N & 1), S = M / 2, np = N * (N + 1) / 2, nblk = S * (S + 1) / 2;
+    zc *P = (zc *)jv_raw;               // packed upper triangle
+    zc *pph = P + np;                   // per pair: the phase of A(p, q)
+    double *pc = (double *)(pph + S);   // c
+    double *ps = pc + S;                // s
+    double *pa = ps + S;                // app after the rotation
+    double *pb = pa + S;                // aqq after the rotation
+    int *sp = (int *)(pb + S);          // the pair of each slot in this round: p
+    int *sq = sp + S;                   //                                      q
+    double *dk = (double *)(sq + S);    // the eigenvalues, for the sort
+    __shared__ double red_off[JV_THREADS / 32], red_tot[JV_THREADS / 32];
+    __shared__ int go;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    // this thread's 2x2 blocks (P1 <= P2 over the slots), the same in every round
+    int task[JV_TASKS];
+    int ntask = 0;
+#pragma unroll
+    for (int u = 0; u < JV_TASKS; u++) {
+        const int t = tid + u * JV_THREADS;
+        task[u] = 0;
+        if (t < nblk) {
+            int P2 = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+            while (P2 * (P2 + 1) / 2 > t) P2--;
+            while ((P2 + 1) * (P2 + 2) / 2 <= t) P2++;
+            task[u] = (P2 << 16) | (t - P2 * (P2 + 1) / 2);
+            ntask = u + 1;
+        }
+    }
+    const zc *a = A + (int64_t)b * N * N;
+    for (int e = tid; e < N * N; e += blockDim.x) {
+        const int i = e % N, j = e / N;
+        if (i < j) P[pk(i, j)] = a[e];
+        else if (i == j) P[pk(i, i)] = zc{a[e].x, 0.0};
+    }
+    const double ne = (double)N * 2.220446049250313e-16;
+    for (int sweep = 0;; sweep++) {
+        __syncthreads();
+        // convergence: off-diagonal weight at rounding level (every thread reads the verdict)
+        double off = 0.0, tot = 0.0;
+        for (int e = tid; e < N * N; e += blockDim.x) {
+            const int i = e % N, j = e / N;
+            if (i > j) continue;
+            const zc v = P[pk(i, j)];
+            const double w = v.x * v.x + v.y * v.y;
+            if (i == j) tot += w;
+            else off += 2.0 * w;
+        }
+        for (int o = 16; o; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if ((tid & 31) == 0) {
+            red_off[tid >> 5] = off;
+            red_tot[tid >> 5] = tot;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            off = 0.0;
+            tot = 0.0;
+            for (int w = 0; w < JV_THREADS / 32; w++) {
+                off += red_off[w];
+                tot += red_tot[w];
+            }
+            tot += off;
+            int g = 1;
+            if (!(off < INFINITY) || !(tot < INFINITY)) g = -1;  // non-finite entries
+            else if (off <= ne * ne * tot) g = 0;
+            else if (sweep >= JAC_MAX_SWEEPS) g = -1;
+            go = g;
+            if (g != 1) info[b] = (g == 0) ? 0 : 1;
+        }
+        __syncthreads();
+        if (go != 1) break;
+        for (int r = 0; r < M - 1; r++) {
+            if (tid < S) {  // the rotation of pair tid (as jac_params)
+                int p, q;
+                jac_slot(M, r, tid, p, q);
+                double c = 1.0, s = 0.0, phx = 1.0, phy = 0.0;
+                double app = P[pk(p, p)].x, aqq = 0.0;
+                if (q < N) {
+                    aqq = P[pk(q, q)].x;
+                    const zc apq = P[pk(p, q)];
+                    const double mag = hypot(apq.x, apq.y);
+                    if (mag > 0.0) {
+                        const double tau = (aqq - app) / (2.0 * mag);
+                        const double tt =
+                            fabs(tau) > 1e150 ? 0.5 / tau : copysign(1.0, tau) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + tt * tt);
+                        s = tt * c;
+                        phx = apq.x / mag;
+                        phy = apq.y / mag;
+                        app -= tt * mag;
+                        aqq += tt * mag;
+                    }
+                }
+                pc[tid] = c;
+                ps[tid] = s;
+                pph[tid] = zc{phx, phy};
+                pa[tid] = app;
+                pb[tid] = aqq;
+                sp[tid] = p;
+                sq[tid] = q;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < JV_TASKS; u++) {  // unrolled: task[] stays in registers
+                if (u >= ntask) break;
+                const int P1 = task[u] & 0xffff, P2 = task[u] >> 16;
+                const int p1 = sp[P1], q1 = sq[P1], p2 = sp[P2], q2 = sq[P2];
+                const bool r2 = q1 < N, c2 = q2 < N;
+                if (P1 == P2) {
+                    if (r2) {
+                        P[pk(p1, p1)] = zc{pa[P1], 0.0};
+                        P[pk(q1, q1)] = zc{pb[P1], 0.0};
+                        P[pk(p1, q1)] = zc{0.0, 0.0};
+                    }
+                    continue;
+                }
+                zc b00 = pget(P, p1, p2), b01{0.0, 0.0}, b10{0.0, 0.0}, b11{0.0, 0.0};
+                if (c2) b01 = pget(P, p1, q2);
+                if (r2) b10 = pget(P, q1, p2);
+                if (r2 && c2) b11 = pget(P, q1, q2);
+                if (r2) {  // rows: p <- c p - s ph q,  q <- s conj(ph) p + c q
+                    const double c = pc[P1], sv = ps[P1];
+                    const zc ph = pph[P1], wm = zc{-sv * ph.x, -sv * ph.y}, wp = zc{sv * ph.x, -sv * ph.y};
+                    zc x0 = c * b00, y0 = c * b10, x1 = c * b01, y1 = c * b11;
+                    cfma(x0, wm, b10);
+                    cfma(y0, wp, b00);
+                    cfma(x1, wm, b11);
+                    cfma(y1, wp, b01);
+                    b00 = x0;
+                    b10 = y0;
+                    b01 = x1;
+                    b11 = y1;
+                }
+                if (c2) {  // columns: p' <- c' p' - s' conj(ph') q',  q' <- s' ph' p' + c' q'
+                    const double c = pc[P2], sv = ps[P2];
+                    const zc ph = pph[P2], wm = zc{-sv * ph.x, sv * ph.y}, wp = zc{sv * ph.x, sv * ph.y};
+                    zc u0 = c * b00, v0 = c * b01, u1 = c * b10, v1 = c * b11;
+                    cfma(u0, wm, b01);
+                    cfma(v0, wp, b00);
+                    cfma(u1, wm, b11);
+                    cfma(v1, wp, b10);
+                    b00 = u0;
+                    b01 = v0;
+                    b10 = u1;
+                    b11 = v1;
+                }
+                pset(P, p1, p2, b00);
+                if (c2) pset(P, p1, q2, b01);
+                if (r2) pset(P, q1, p2, b10);
+                if (r2 && c2) pset(P, q1, q2, b11);
+            }
+            __syncthreads();
+        }
+    }
+    // eigenvalues ascending (the order of jac_sort)
+    for (int i = tid; i < N; i += blockDim.x) dk[i] = P[pk(i, i)].x;
+    __syncthreads();
+    for (int i = tid; i < N; i += blockDim.x) {
+        const double di = dk[i];
+        const bool ni = isnan(di);
+        const double ki = ni ? INFINITY : di;
+        int k = 0;
+        for (int j = 0; j < N; j++) {
+            const double dj = dk[j];
+            const bool nj = isnan(dj);
+            const double kj = nj ? INFINITY : dj;
+            k += kj < ki || (kj == ki && (nj < ni || (nj == ni && j < i)));
+        }
+        E[(int64_t)b * N + k] = di;
+    }
+}
+
 // ---- Loewdin transform ----
 
 // C = alpha A op(B) + beta C, complex FP64, column-major, op(B) = B or B^H; 64x64 tiles of C,
@@ -495,6 +694,54 @@ int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, 
         (e = cudaMemcpyAsync(E, dE, sizeof(double) * (size_t)N * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
         (e = cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
         e = cudaStreamSynchronize(st);
+    if (dA) cudaFreeAsync(dA, st);
+    if (dW) cudaFreeAsync(dW, st);
+    if (dE) cudaFreeAsync(dE, st);
+    if (dinfo) cudaFreeAsync(dinfo, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return -(int)e;
+    int bad = 0;
+    for (int b = 0; b < batch; b++) {
+        if (info) info[b] = hinfo[b];
+        bad |= hinfo[b];
+    }
+    return bad ? 1 : 0;
+}
+
+int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *info, int device) {
+    if (N < 1 || N > JAC_MAX_N || batch < 0 || batch > 65535 || (batch > 0 && (!A || !E))) return -1;
+    if (batch == 0) return 0;
+    DeviceScope ds(device);
+    if (ds.err != cudaSuccess) return -(int)ds.err;
+    const size_t nn = (size_t)N * N * batch;
+    cudaStream_t st = nullptr;
+    zc *dA = nullptr, *dW = nullptr;
+    double *dE = nullptr;
+    int *dinfo = nullptr;
+    std::vector<int> hinfo(batch, 0);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return -(int)e;
+    const bool small = N <= JV_MAX_N;
+    if ((e = cudaMallocAsync(&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (small || (e = cudaMallocAsync(&dW, sizeof(zc) * nn, st)) == cudaSuccess) &&
+        (e = cudaMallocAsync(&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
+        (e = cudaMallocAsync(&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess) {
+        if (small) {
+            if ((e = smem_cap((const void *)jac_values)) == cudaSuccess) {
+                jac_values<<<batch, JV_THREADS, jv_smem(N), st>>>(N, dA, dE, dinfo);
+                count_launch();
+                e = cudaGetLastError();
+            }
+        } else {
+            e = eigh_dev(st, N, batch, dA, dE, dinfo, dW);  // the eigenvectors are not used
+        }
+        if (e == cudaSuccess &&
+            (e = cudaMemcpyAsync(E, dE, sizeof(double) * (size_t)N * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
+            (e = cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+    }
     if (dA) cudaFreeAsync(dA, st);
     if (dW) cudaFreeAsync(dW, st);
     if (dE) cudaFreeAsync(dE, st);

@@ -16,7 +16,7 @@ int main(int argc, char **argv) {
     api.solve_scf = (int (*)(void *, double, int, qs_scf_result *))qs_solve_scf;
     api.current = (int (*)(void *, double, double *, double *))qs_current;
     api.get_observables = (int (*)(void *, double *, double *, double *, double *))qs_get_observables;
-    api.hermitian_eigensystem = qs_hermitian_eigensystem;
+    api.hermitian_eigenvalues = qs_hermitian_eigenvalues;
     api.dftb_lowdin = qs_dftb_lowdin;
     const char *dev = std::getenv("QS_DEVICE");
     return qsh_run(argc > 1 ? argv[1] : ".", &api, QS_PREC_FP64, dev ? std::atoi(dev) : 0, stdout);

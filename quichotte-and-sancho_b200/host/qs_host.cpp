@@ -1073,13 +1073,12 @@ struct Model {
 
     // src/quichotte.f90:241-253 energy grid from the spectrum of H
     void energy_grid() {
-        if (api && api->hermitian_eigensystem) {
-            std::vector<cplx> A = H;
+        if (api && api->hermitian_eigenvalues) {
             Ev.assign(Norb, 0.0);
             int info = 0;
-            int rc = api->hermitian_eigensystem(Norb, 1, (double *)A.data(), Ev.data(), &info, device);
+            int rc = api->hermitian_eigenvalues(Norb, 1, (const double *)H.data(), Ev.data(), &info, device);
             if (rc == 1) fail(" ERROR: ZHEEV eigenproblem failed, INFO = " + std::to_string(info));
-            if (rc != 0) fail(" ERROR: device set-up failed (hermitian_eigensystem status " + std::to_string(rc) + ")");
+            if (rc != 0) fail(" ERROR: device set-up failed (hermitian_eigenvalues status " + std::to_string(rc) + ")");
         } else {
             std::vector<cplx> Z;
             jacobi_herm(Norb, H, Ev, Z);

@@ -92,7 +92,7 @@ RESIDUAL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, _dp, _dp, 
 
 _host.qsh_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(_QshModel)), ctypes.c_char_p, ctypes.c_int,
                            ctypes.c_void_p]
-EIGENSYSTEM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int)
+EIGENVALUES_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int)
 LOWDIN_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int)
 
 
@@ -102,7 +102,7 @@ class QshSolverApi(ctypes.Structure):
     _fields_ = ([("name", ctypes.c_char_p)] + [(k, ctypes.c_void_p) for k in ("create", "destroy", "last_error",
                                                                               "solve_scf", "current",
                                                                               "get_observables")]
-                + [("hermitian_eigensystem", EIGENSYSTEM_FN), ("dftb_lowdin", LOWDIN_FN)])
+                + [("hermitian_eigenvalues", EIGENVALUES_FN), ("dftb_lowdin", LOWDIN_FN)])
 
 
 _host.qsh_load_with.argtypes = [ctypes.c_char_p, ctypes.POINTER(QshSolverApi), ctypes.c_int,
@@ -161,7 +161,7 @@ C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current
          "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
          "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
          "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice",
-         "qs_hermitian_eigensystem", "qs_dftb_lowdin")
+         "qs_hermitian_eigensystem", "qs_hermitian_eigenvalues", "qs_dftb_lowdin")
 TUNE_DYSON, TUNE_KELDYSH, TUNE_SIG2_A, TUNE_SIG2_C = 0, 1, 2, 3
 QS_ERR_NOALLOC_LIMIT = -1001
 QS_ERR_TOO_LARGE = -1002
@@ -213,6 +213,8 @@ _lib.qs_server_destroy.restype = None
 _lib.qs_invert_batched_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p]
 _lib.qs_hermitian_eigensystem.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_int]
+_lib.qs_hermitian_eigenvalues.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_int]
 _lib.qs_dftb_lowdin.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                 ctypes.c_void_p, _dp, ctypes.c_int]
@@ -492,6 +494,23 @@ def hermitian_eigensystem(A, device=0):
         raise SolverError(f"hermitian_eigensystem failed ({rc})")
     Z = buf.transpose(0, 2, 1).copy()
     return (E[0], Z[0], info[0]) if single else (E, Z, info)
+
+
+def hermitian_eigenvalues(A, device=0):
+    """Eigenvalues only (zheev JOBZ='N') on the device. A: (batch, N, N) or (N, N) Hermitian
+    complex, not modified. Returns (E ascending, info)."""
+    A = np.asarray(A, np.complex128)
+    single = A.ndim == 2
+    if single:
+        A = A[None]
+    batch, N, _ = A.shape
+    buf = np.array(A.transpose(0, 2, 1), dtype=np.complex128, order="C", copy=True)
+    E = np.zeros((batch, N))
+    info = np.zeros(batch, np.int32)
+    rc = _lib.qs_hermitian_eigenvalues(N, batch, _ptr(buf), _ptr(E), _ptr(info), device)
+    if rc < 0:
+        raise SolverError(f"hermitian_eigenvalues failed ({rc})")
+    return (E[0], info[0]) if single else (E, info)
 
 
 def dftb_lowdin(S, H0, Lam, soc_dual=True, device=0):

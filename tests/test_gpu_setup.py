@@ -1,6 +1,7 @@
 """The set-up's dense linear algebra on the device against LAPACK (numpy) restatements.
 
-- qs_hermitian_eigensystem replaces hermitian_eigensystem (common/linear_algebra.f90:32-56,
+- qs_hermitian_eigensystem (and qs_hermitian_eigenvalues, without vectors) replace
+  hermitian_eigensystem (common/linear_algebra.f90:32-56,
   zheev): eigenvalues within 1e-12 ||A||_2 of numpy.linalg.eigh (LAPACK), eigenvectors by
   their residual ||A Z - Z E|| and orthonormality (a degenerate eigenvalue's basis is not
   unique, so the subspace projector is compared instead of the vectors).
@@ -125,3 +126,39 @@ def test_dftb_lowdin_refuses_indefinite_overlap():
     S[0, 1] = S[1, 0] = 1.5  # eigenvalues 1 +- 1.5
     with pytest.raises(qb.SolverError, match="not positive definite"):
         qb.dftb_lowdin(S, np.zeros((N, N)), np.zeros((2 * N, 2 * N), complex))
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 16, 17, 64, 120, 129, 160, 161, 248])
+def test_eigenvalues_only_random_batch(N):
+    # N <= 160: one block per matrix with the matrix in shared memory; above: the sweep graphs
+    rng = np.random.default_rng(300 + N)
+    A = np.stack([_herm(rng, N, s) for s in (1.0, 1e-3, 50.0)])
+    A0 = A.copy()
+    E, info = qb.hermitian_eigenvalues(A)
+    assert list(info) == [0, 0, 0]
+    assert np.array_equal(A, A0)
+    for b in range(3):
+        En = np.linalg.eigvalsh(A[b])
+        assert np.all(np.diff(E[b]) >= 0)
+        assert np.max(np.abs(E[b] - En)) <= TOL * max(1.0, np.max(np.abs(En)))
+
+
+def test_eigenvalues_only_edge_cases_and_helix():
+    N = 7
+    diag = np.diag([3.0, -1.0, 2.0, -1.0, 0.5, 7.0, -4.0]).astype(complex)
+    nan = _herm(np.random.default_rng(9), N)
+    nan[1, 5] = np.nan
+    nan[5, 1] = np.nan
+    ok = _herm(np.random.default_rng(10), N)
+    E, info = qb.hermitian_eigenvalues(np.stack([np.zeros((N, N), complex), diag, nan, ok]))
+    assert list(info) == [0, 0, 1, 0]
+    assert np.all(E[0] == 0)
+    assert np.array_equal(E[1], np.sort(np.diag(diag).real))
+    assert np.max(np.abs(E[3] - np.linalg.eigvalsh(ok))) <= TOL * np.max(np.abs(E[3]))
+    m = qb.Model.helix(N_ions=10, N_turns=6, hel_length=0.34 * 6 * 9 / 10, hel_radius=0.7, hand=1.0, E_CC=0.0,
+                       t_hop=1.0, lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0,
+                       mu=0.0, dw=2.0, up=2.0, delta=0.01)
+    Eh, infoh = qb.hermitian_eigenvalues(m.H)
+    assert infoh == 0
+    assert np.max(np.abs(Eh - np.linalg.eigvalsh(m.H))) <= TOL * np.max(np.abs(Eh))
+    assert np.max(np.abs(Eh - m.Ev)) <= TOL * np.max(np.abs(Eh))  # the host's Jacobi
