@@ -70,6 +70,30 @@ __global__ void jac_init(int N, int64_t total, zc *__restrict__ A, zc *__restric
     }
 }
 
+// Scale matrix b by 2^-e[b] so that its largest |Re| or |Im| lies in [1, 2): exact, and the
+// sums of squares of the convergence test neither overflow nor underflow (LAPACK scales
+// likewise). The eigenvalues are scaled back by 2^e[b]; the eigenvectors do not change.
+// One block per matrix.
+__global__ void jac_scale(int N, zc *__restrict__ A, int *__restrict__ expo) {
+    const int b = blockIdx.x;
+    zc *a = A + (int64_t)b * N * N;
+    double m = 0.0;
+    for (int64_t e = threadIdx.x; e < (int64_t)N * N; e += blockDim.x) m = fmax(m, fmax(fabs(a[e].x), fabs(a[e].y)));
+    __shared__ double sm[32];
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sm[w]);
+    const int ex = (m > 0.0 && m < INFINITY) ? ilogb(m) : 0;  // NaN or Inf: left to the test
+    if (threadIdx.x == 0) expo[b] = ex;
+    if (ex == 0) return;
+    for (int64_t e = threadIdx.x; e < (int64_t)N * N; e += blockDim.x) {
+        a[e].x = ldexp(a[e].x, -ex);
+        a[e].y = ldexp(a[e].y, -ex);
+    }
+}
+
 // done[b]: 0 active, 1 converged, 2 not finite (stops; reported as not converged).
 // One block per matrix; counts the active matrices into *active.
 __global__ void jac_check(int N, const zc *__restrict__ A, int *__restrict__ done, int *__restrict__ active) {
@@ -224,7 +248,8 @@ __global__ void __launch_bounds__(JAC_THREADS) jac_rotate(int N, int M, int G, z
 
 // eigenvalues ascending (ties and non-finite values in index order, NaN last) and the rank of
 // every diagonal entry; one block per matrix
-__global__ void jac_sort(int N, const zc *__restrict__ A, double *__restrict__ E, int *__restrict__ rank) {
+__global__ void jac_sort(int N, const zc *__restrict__ A, const int *__restrict__ expo, double *__restrict__ E,
+                         int *__restrict__ rank) {
     extern __shared__ double dk[];
     const int b = blockIdx.x;
     const zc *a = A + (int64_t)b * N * N;
@@ -247,7 +272,7 @@ __global__ void jac_sort(int N, const zc *__restrict__ A, double *__restrict__ E
             k += before;
         }
         rank[(int64_t)b * N + i] = k;
-        E[(int64_t)b * N + k] = di;
+        E[(int64_t)b * N + k] = ldexp(di, expo[b]);
     }
 }
 
@@ -270,7 +295,7 @@ int grid_for(int64_t total) { return (int)std::max<int64_t>(1, std::min<int64_t>
 cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int *dinfo, zc *dW) {
     const int M = N + (N & 1), S = M / 2;
     const int64_t total = (int64_t)N * N * batch;
-    int *dflag = nullptr, *dact = nullptr, *drank = nullptr;
+    int *dflag = nullptr, *dact = nullptr, *drank = nullptr, *dexpo = nullptr;
     JacPair *dpairs = nullptr;
     JacRow *drows = nullptr;
     cudaGraph_t graph = nullptr;
@@ -288,8 +313,9 @@ cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int 
     do {                                    \
         if ((e = (x)) != cudaSuccess) goto out; \
     } while (0)
-    JAC_TRY(cudaMallocAsync(&dflag, sizeof(int) * (batch + 1), st));
+    JAC_TRY(cudaMallocAsync(&dflag, sizeof(int) * (2 * batch + 1), st));
     dact = dflag + batch;
+    dexpo = dact + 1;
     JAC_TRY(cudaMallocAsync(&drank, sizeof(int) * (size_t)N * batch, st));
     JAC_TRY(cudaMallocAsync(&dpairs, sizeof(JacPair) * (size_t)S * batch, st));
     JAC_TRY(cudaMallocAsync(&drows, sizeof(JacRow) * (size_t)M * batch, st));
@@ -297,6 +323,8 @@ cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int 
     JAC_TRY(smem_cap((const void *)jac_sort));
     JAC_TRY(cudaMemsetAsync(dflag, 0, sizeof(int) * (batch + 1), st));
     jac_init<<<grid_for(total), 256, 0, st>>>(N, total, dA, dW);
+    count_launch();
+    jac_scale<<<batch, 256, 0, st>>>(N, dA, dexpo);
     count_launch();
     jac_check<<<batch, 256, 0, st>>>(N, dA, dflag, dact);
     count_launch();
@@ -323,7 +351,7 @@ cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int 
             sweeps++;
         }
     }
-    jac_sort<<<batch, 256, sizeof(double) * N, st>>>(N, dA, dE, drank);
+    jac_sort<<<batch, 256, sizeof(double) * N, st>>>(N, dA, dexpo, dE, drank);
     count_launch();
     jac_permute<<<grid_for(total), 256, 0, st>>>(N, total, dW, drank, dA);
     count_launch();
@@ -389,7 +417,7 @@ __global__ void __launch_bounds__(JV_THREADS) jac_values(int N, const zc *__rest
     int *sq = sp + S;                   //                                      q
     double *dk = (double *)(sq + S);    // the eigenvalues, for the sort
     __shared__ double red_off[JV_THREADS / 32], red_tot[JV_THREADS / 32];
-    __shared__ int go;
+    __shared__ int go, ex_s;
     const int b = blockIdx.x, tid = threadIdx.x;
     // this thread's 2x2 blocks (P1 <= P2 over the slots), the same in every round
     int task[JV_TASKS];
@@ -411,6 +439,23 @@ __global__ void __launch_bounds__(JV_THREADS) jac_values(int N, const zc *__rest
         const int i = e % N, j = e / N;
         if (i < j) P[pk(i, j)] = a[e];
         else if (i == j) P[pk(i, i)] = zc{a[e].x, 0.0};
+    }
+    __syncthreads();
+    {  // scale by 2^-ex so that the largest |Re| or |Im| lies in [1, 2) (as jac_scale)
+        double m = 0.0;
+        for (int e = tid; e < np; e += blockDim.x) m = fmax(m, fmax(fabs(P[e].x), fabs(P[e].y)));
+        for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((tid & 31) == 0) red_off[tid >> 5] = m;
+        __syncthreads();
+        if (tid == 0) {
+            m = 0.0;
+            for (int w = 0; w < JV_THREADS / 32; w++) m = fmax(m, red_off[w]);
+            ex_s = (m > 0.0 && m < INFINITY) ? ilogb(m) : 0;
+        }
+        __syncthreads();
+        const int ex = ex_s;
+        if (ex != 0)
+            for (int e = tid; e < np; e += blockDim.x) P[e] = zc{ldexp(P[e].x, -ex), ldexp(P[e].y, -ex)};
     }
     const double ne = (double)N * 2.220446049250313e-16;
     for (int sweep = 0;; sweep++) {
@@ -548,7 +593,7 @@ __global__ void __launch_bounds__(JV_THREADS) jac_values(int N, const zc *__rest
             const double kj = nj ? INFINITY : dj;
             k += kj < ki || (kj == ki && (nj < ni || (nj == ni && j < i)));
         }
-        E[(int64_t)b * N + k] = di;
+        E[(int64_t)b * N + k] = ldexp(di, ex_s);
     }
 }
 

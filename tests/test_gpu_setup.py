@@ -162,3 +162,20 @@ def test_eigenvalues_only_edge_cases_and_helix():
     assert infoh == 0
     assert np.max(np.abs(Eh - np.linalg.eigvalsh(m.H))) <= TOL * np.max(np.abs(Eh))
     assert np.max(np.abs(Eh - m.Ev)) <= TOL * np.max(np.abs(Eh))  # the host's Jacobi
+
+
+@pytest.mark.parametrize("scale", [1e250, 1e-250])
+def test_extreme_scales_as_lapack(scale):
+    # |a|^2 would overflow (or underflow) in the convergence test: both paths scale the
+    # matrix by an exact power of two first, as LAPACK does
+    rng = np.random.default_rng(21)
+    A = np.stack([_herm(rng, N=40, scale=scale), _herm(rng, N=40, scale=scale)])
+    En = np.linalg.eigvalsh(A)
+    E1, Z, info1 = qb.hermitian_eigensystem(A)
+    E2, info2 = qb.hermitian_eigenvalues(A)
+    assert list(info1) == [0, 0] and list(info2) == [0, 0]
+    for b in range(2):
+        nrm = np.max(np.abs(En[b]))
+        assert np.max(np.abs(E1[b] - En[b])) <= TOL * nrm
+        assert np.max(np.abs(E2[b] - En[b])) <= TOL * nrm
+        assert np.max(np.abs(Z[b].conj().T @ Z[b] - np.eye(40))) <= 10 * TOL
