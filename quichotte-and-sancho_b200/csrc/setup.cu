@@ -1,8 +1,11 @@
 // setup.cu -- the dense linear algebra of the model set-up, on the device.
 //
 //   qs_hermitian_eigensystem  hermitian_eigensystem (common/linear_algebra.f90:32-56, LAPACK
-//                             zheev) over a batch of matrices of one size; the program calls
-//                             it for the energy grid (src/quichotte.f90:79-83).
+//                             zheev) over a batch of matrices of one size.
+//   qs_hermitian_eigenvalues  the same without eigenvectors (zheev JOBZ = 'N'), which is all
+//                             the energy grid needs (src/quichotte.f90:79-83): for N <= 160
+//                             one block per matrix with the matrix in shared memory
+//                             (jac_values below).
 //   qs_dftb_lowdin            the dense part of build_hamiltonian_from_dftb_hs
 //                             (src/hamiltonian.f90:625-640, 680-689): S^-1/2 from the
 //                             eigenpairs of S (dsyev there), the SOC form on the spin-doubled
@@ -20,7 +23,8 @@
 // of a sweep and the convergence test are one CUDA graph, replayed once per sweep; the host
 // reads one counter per sweep. A matrix is converged when its off-diagonal weight is at
 // rounding level, sum_{i!=j} |a_ij|^2 <= (N eps)^2 sum |a_ij|^2; then every eigenvalue is
-// within about N eps ||A||_F of the exact one, the accuracy class of zheev.
+// within about N eps ||A||_F of the exact one, the accuracy class of zheev. Each matrix is
+// first scaled by an exact power of two (jac_scale), so the sums of squares stay in range.
 #include <cmath>
 #include <cstdio>
 #include <vector>
