@@ -6,20 +6,23 @@ continuation from the previous one, then Current and the observables):
   SOC lambda = 0.01 eV, radius 0.7 nm, pitch 0.34 nm/turn, hand = +1, wide-band leads
   Gamma_L = Gamma_R = 0.5 eV on the first and last site, U = 1.0 eV on every site,
   2nd order, T = 300 K, mu = 0, 16384 energies on [-12, 12] eV, V from -1 to 1 V in
-  steps of 0.05 V (41 voltages), Broyden: reference defaults (alpha_mix 0.5, 16-column
-  single-precision history, tolf 1e-6). Synthetic input (the model is analytic).
+  steps of 0.05 V (41 voltages), Broyden: the reference's input defaults (alpha_mix 0.5,
+  16-column single-precision history, tolf 1e-6, maxscf 300). Synthetic input (the model
+  is analytic).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--precision both|fp64|mixed]
                   [--serve R] [--serve-rate r] [--serve-inflight k]
 
 Default: the FP64 form, then the mixed form (the headline value), their ratio and the
-current error of the mixed form against the FP64 one; then a serving stream (p50/p99
-latency of IV-point requests through qs_server).
+error of every observable of the mixed form against the FP64 one over the points both
+converged; the CPU oracle on a bounded sample of the same sweep beside the GPU on the same
+sample; then a serving stream (p50/p99 latency of IV-point requests through qs_server).
 
 N > 1 (launched with torch.distributed.run): replicas. Rank r solves its own contiguous
 block of the voltage sweep; no data-path collective. value = all IV points / max over
-ranks of the device time. The reference arm (--impl reference) times the CPU oracle
-(a restatement of the reference's Fortran path) on the host cores.
+ranks of the device time. The reference arm (--impl reference) times the CPU oracle (a
+restatement of the reference's Fortran path, oracle/) on the host cores; it loads the
+oracle's library only.
 """
 import argparse
 import json
@@ -57,7 +60,8 @@ def model_cfg1(qb, n_omega=N_OMEGA, ions=N_IONS, turns=N_TURNS):
         up += 0.5 * delta
         m = qb.Model.helix(dw=dw, up=up, delta=delta, **args)
     assert m.n_omega == n_omega, m.n_omega
-    m.alpha_mix, m.nhist, m.tolf, m.maxscf, m.single_history = 0.5, 16, 1e-6, 300, True
+    m.alpha_mix, m.nhist, m.tolf, m.maxscf = BROYDEN["alpha_mix"], BROYDEN["nhist"], BROYDEN["tolf"], BROYDEN["maxscf"]
+    m.single_history = bool(BROYDEN["single_history"])
     return m
 
 
@@ -114,32 +118,118 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-# SCF steps per IV point of this workload, measured on B200 (both arms run the same
-# Broyden algorithm, so the oracle takes the same number of steps up to rounding)
-STEPS_PER_POINT = 25.5
+# Broyden settings of the workload: the reference's input defaults (src/input_output.f90:
+# 109-114). Both arms and every form use them.
+BROYDEN = dict(alpha_mix=0.5, nhist=16, tolf=1e-6, maxscf=300, single_history=1)
+# energies of the CPU sample grid (the same helix and window; see cpu_sample_sweep)
+SAMPLE_N = 512
 
 
-def cpu_baseline_sample(n_sample=4096, steps_per_point=STEPS_PER_POINT, threads=None):
-    """The CPU oracle on a bounded sample of the workload: one SCF step (scf_residual2:
-    Sigma2 by FFT + the Dyson/Keldysh sweep) of the same helix on the same energy window
-    with n_sample energies, scaled linearly to the 16384-energy grid and multiplied by the
-    SCF steps of one IV point. The Broyden update is left out (in the CPU's favour)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-    import quichotte_b200 as qb
-    m = model_cfg1(qb, n_sample)
-    s = oracle_lib.solver(m, nhist=0)
-    x = s.initial_vector(VOLTS[0])
-    t0 = time.perf_counter()
-    F, ab = s.residual(VOLTS[0], x)
-    dt = time.perf_counter() - t0
+def bench_config(n_omega, ions, turns, nhist, world):
+    """The static description of the workload, identical in every arm's line."""
+    N = 2 * ions * turns
+    b = dict(BROYDEN, nhist=nhist)
+    return {"workload": f"helix {ions}x{turns} ({N}x{N} complex), {n_omega} energies on [-12,12] eV, order 2, "
+                        "U=1.0 eV, lambda=0.01 eV, Gamma_L=Gamma_R=0.5 eV, T=300 K; V sweep -1..1 V step 0.05 "
+                        "with continuation; the first W voltages warm up, the next K are timed",
+            "broyden": {"alpha_mix": b["alpha_mix"], "nhist": b["nhist"], "history": "single" if b["single_history"]
+                        else "double", "tolf": b["tolf"], "maxscf": b["maxscf"]},
+            "forms": "FP64 GPU form, then the mixed form (headline)",
+            "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 126 MB (no flush needed)"}
+
+
+def cpu_sample_sweep(volts, n_sample=SAMPLE_N, threads=None, ions=N_IONS, turns=N_TURNS):
+    """The CPU oracle (oracle/oracle_py.py: the model built in numpy, only liboracle.so loaded)
+    on a bounded sample of the sweep: real converged IV points of the same helix, physics,
+    window and Broyden settings at the voltages `volts` (continuation from the first, fresh
+    after an unconverged point, as src/quichotte.f90:125-143), on a grid of n_sample energies
+    instead of 16384. Returns per-point wall times, step counts and currents."""
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    m = oracle_py.Helix(ions, turns, PITCH * turns * (ions - 1) / ions, RADIUS, 1.0, 0.0, 1.0, 0.01, 1.0, 0.5, 0.5,
+                        0.5, 300.0, 0.0, W_LO, (W_HI - W_LO) / n_sample, n_sample)
+    s = oracle_py.Solver(m, **BROYDEN)
+    out, ok = [], False
+    for k, V in enumerate(volts):
+        r = s.solve_scf(V, k == 0 or not ok)
+        ok = r["converged"]
+        out.append(dict(V=V, converged=ok, n_iter=r["n_iter"], wall=r["wall"], J=s.current(V)))
     s.close()
-    scale = N_OMEGA / n_sample
-    per_point = dt * scale * steps_per_point
-    return {"value": 1.0 / per_point, "unit": "IV points/s", "cores": threads or os.cpu_count(), "kind": "port",
-            "sample": f"CPU oracle (OpenMP, OpenBLAS zgetrf/zgetri, own FFT), one scf_residual2 of the same helix "
-                      f"on {n_sample} energies over [-12,12] eV: {dt:.2f} s; x{scale:g} to 16384 energies and "
-                      f"x{steps_per_point:g} SCF steps per IV point; Broyden update not counted"}
+    return out
+
+
+def scaled_cpu_rate(points, n_sample):
+    """IV points/s of the 16384-energy workload from the sample: converged sample points per
+    second x n_sample/16384 (the Dyson, Keldysh and Broyden work per SCF step is linear in the
+    number of energies and the FFT's n log n only slightly more, so this favours the CPU)."""
+    t = sum(p["wall"] for p in points)
+    conv = sum(int(p["converged"]) for p in points)
+    rate = conv / t if t > 0 else 0.0
+    return rate * n_sample / N_OMEGA, rate, t, conv
+
+
+def cpu_baseline_line(qb, volts, n_sample, ions, turns, device):
+    """cpu_baseline of the GPU arm's line: the CPU oracle on a bounded sample (the first
+    timed voltages, on the sample grid), and the GPU's FP64 form on exactly the same sample
+    points in the same run (device time and wall time), so that the two are compared on
+    identical work as well as through the scaled figure."""
+    nthr = os.cpu_count()
+    pts = cpu_sample_sweep(volts, n_sample, threads=nthr, ions=ions, turns=turns)
+    v, v_sample, t, conv = scaled_cpu_rate(pts, n_sample)
+    ms = model_cfg1(qb, n_sample, ions, turns)
+    s = qb.Solver(ms, device=device, **BROYDEN)
+    gdev, gwall, gconv, giters, gJ, ok = 0.0, 0.0, 0, [], [], False
+    for k, V in enumerate(volts):
+        t0 = time.perf_counter()
+        r = s.solve_scf(V, k == 0 or not ok)
+        J = s.current(V)
+        s.observables()
+        gwall += time.perf_counter() - t0
+        ok = r["converged"]
+        gdev += r["seconds"]
+        gconv += int(ok)
+        giters.append(r["n_iter"])
+        gJ.append(J)
+    s.close()
+    jc = np.array([p["J"] for p in pts])
+    jg = np.array(gJ)
+    return {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port",
+            "sample": f"CPU oracle (OpenMP over energies, OpenBLAS zgetrf/zgetri/dposv, radix-4 FFT; oracle/) on "
+                      f"{nthr} threads: real converged IV points of the same sweep at V = {volts[0]:g}..{volts[-1]:g} "
+                      f"(fresh start at the first) on {n_sample} energies over [-12,12] eV; value = the sample's "
+                      f"IV points/s x{n_sample}/{N_OMEGA}",
+            "sample_value": v_sample, "sample_s": t, "sample_converged": conv, "sample_energies": n_sample,
+            "scf_steps_per_point": [p["n_iter"] for p in pts],
+            "gpu_same_sample": {"form": "fp64", "device_s": gdev, "wall_s": gwall, "converged": gconv,
+                                "scf_steps_per_point": giters,
+                                "value": gconv / gdev if gdev > 0 else 0.0, "e2e": gconv / gwall if gwall > 0 else 0.0,
+                                "current_rel_diff_vs_cpu": float(np.max(np.abs(jg - jc)) / np.max(np.abs(jc)))}}
+
+
+def observable_errors(ref_pts, pts):
+    """Error of every observable of `pts` against `ref_pts` (the FP64 form), over the
+    points that converged in both: currents relative to the largest |J| of the compared
+    points (J crosses zero in the sweep), occupations and the spectral function relative to
+    their largest magnitude at each point. Points that either form did not converge are
+    excluded and counted."""
+    both = [k for k in range(min(len(ref_pts), len(pts))) if ref_pts[k]["converged"] and pts[k]["converged"]]
+    out = {"points_compared": len(both), "points_excluded_not_converged": len(pts) - len(both)}
+    if not both:
+        return out
+    jr = np.array([ref_pts[k]["J"] for k in both])
+    jm = np.array([pts[k]["J"] for k in both])
+    out["current_rel"] = float(np.max(np.abs(jm - jr)) / np.max(np.abs(jr)))
+    occ = max(float(np.max(np.abs(pts[k]["occ"] - ref_pts[k]["occ"])) / np.max(np.abs(ref_pts[k]["occ"])))
+              for k in both)
+    G = max(float(np.max(np.abs(pts[k]["G"] - ref_pts[k]["G"])) / np.max(np.abs(ref_pts[k]["G"]))) for k in both)
+    spec = max(float(np.max(np.abs(pts[k]["dosd"] - ref_pts[k]["dosd"])) / np.max(np.abs(ref_pts[k]["dosd"])))
+               for k in both)
+    out.update(occupation_rel=occ, G_less_obs_rel=G, spectral_rel=spec,
+               current_rel_per_point=[float(np.max(np.abs(np.array(pts[k]["J"]) - np.array(ref_pts[k]["J"])))
+                                            / np.max(np.abs(jr))) for k in both])
+    return out
 
 
 def voltage_block(rank, world, volts=VOLTS):
@@ -213,27 +303,37 @@ def run_serving(qb, n_req, rate, max_inflight, precision):
 
 def run_reference(args, rank, world):
     """--impl reference: the oracle (a restatement of the reference's CPU path: OpenMP
-    over energies, LAPACK zgetrf/zgetri from OpenBLAS, its own FFT) on the host cores."""
+    over energies, LAPACK zgetrf/zgetri from OpenBLAS, its own FFT; oracle/) on all host
+    cores. Each step is a bounded sample of the workload: one real converged IV point of the
+    same sweep (same voltage, continuation, model, window and Broyden settings) on a grid of
+    --ref-sample energies. The line's value scales the measured rate to the 16384-energy
+    grid (scaled_cpu_rate); ms_per_step is the measured time of a sample step."""
     if rank != 0:
         return 0
     nthr = os.cpu_count()
-    os.environ.setdefault("OMP_NUM_THREADS", str(nthr))
-    times = []
-    for k in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        cb = cpu_baseline_sample(args.ref_sample, threads=nthr)
-        if k >= args.warmup:
-            times.append(1.0 / cb["value"])
-    t = sum(times)
-    v = args.steps / t
+    ions, turns = (int(v) for v in args.helix.split("x"))
+    block = voltage_block(0, 1)
+    seq = block[:args.warmup + args.steps]
+    t0 = time.perf_counter()
+    pts = cpu_sample_sweep(seq, args.ref_sample, threads=nthr, ions=ions, turns=turns)
+    timed = pts[args.warmup:]
+    v, v_sample, t, conv = scaled_cpu_rate(timed, args.ref_sample)
+    desc = (f"CPU oracle (OpenMP over energies, OpenBLAS zgetrf/zgetri/dposv, radix-4 FFT; oracle/) on {nthr} "
+            f"threads: {len(timed)} real converged IV points of the same sweep (voltages {timed[0]['V']:g}.."
+            f"{timed[-1]['V']:g}, continuation after {args.warmup} warm-up points) on {args.ref_sample} energies "
+            f"over [-12,12] eV: {conv} converged in {t:.1f} s = {v_sample:.4g} IV points/s; x{args.ref_sample}/"
+            f"{N_OMEGA} to the 16384-energy grid")
     line = {"metric": "converged IV points/s", "value": v, "unit": "IV points/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / max(len(timed), 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "helix 10x6 (120x120), 16384 energies on [-12,12] eV, order 2, U=1.0 eV, "
-                                   "V sweep -1..1 V step 0.05"},
-            "cpu_baseline": {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port", "sample": cb["sample"]},
-            "e2e": {"value": v, "unit": "IV points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": bench_config(args.n_omega, ions, turns, args.nhist, world),
+            "cpu_baseline": {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port", "sample": desc,
+                             "sample_value": v_sample, "sample_energies": args.ref_sample,
+                             "scf_steps_per_point": [p["n_iter"] for p in timed],
+                             "converged": [bool(p["converged"]) for p in timed]},
+            "e2e": {"value": v, "unit": "IV points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "run_s": time.perf_counter() - t0}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -344,9 +444,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-sample", type=int, default=4096)
+    ap.add_argument("--ref-sample", type=int, default=SAMPLE_N, help="energies of the CPU sample grid")
+    ap.add_argument("--cpu-points", type=int, default=3, help="timed voltages in the GPU arm's CPU sample")
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
-    ap.add_argument("--nhist", type=int, default=16, help="smaller histories for profiling only")
+    ap.add_argument("--nhist", type=int, default=BROYDEN["nhist"], help="smaller histories for profiling only")
     ap.add_argument("--helix", default=f"{N_IONS}x{N_TURNS}", help="sites/turn x turns; other sizes for profiling only")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: time kernel variants per size (default); 2/3: force variant 1/2 (profiling only)")
@@ -386,12 +487,12 @@ def main():
     seq = [block[k % len(block)] for k in range(args.warmup + args.steps)]
     fresh = [k == 0 or (k % len(block) == 0) for k in range(len(seq))]
     obs_bytes = 8 * (2 * m.Norb * m.Norb + m.Norb * m.n_omega + 2 * m.n_omega)
+    settings = dict(BROYDEN, nhist=args.nhist)
 
     def run_arm(precision):
         """warm-up + timed IV points of one solver form; the two forms do not fit in HBM
         together, so each arm creates and releases its own solver"""
-        solver = qb.Solver(m, precision=precision, device=local, alpha_mix=0.5, nhist=args.nhist, tolf=1e-6,
-                           maxscf=300, single_history=1)
+        solver = qb.Solver(m, precision=precision, device=local, **settings)
         prev_ok = False
         for k in range(args.warmup):
             # continuation as the reference's sweep: fresh after an unconverged voltage
@@ -406,21 +507,22 @@ def main():
         clocks.start()
         solver.profile(True)
         l0 = qb.kernel_launches()
-        dev_s, n_conv, iters, mixed_steps, currents = 0.0, 0, [], [], []
+        dev_s, points = 0.0, []
         wall0 = time.perf_counter()
         for k in range(args.warmup, args.warmup + args.steps):
             r = solver.solve_scf(seq[k], fresh[k] or not prev_ok)
             prev_ok = r["converged"]
             dev_s += r["seconds"]
-            n_conv += int(r["converged"])
-            iters.append(r["n_iter"])
-            mixed_steps.append(r["n_mixed"])
-            currents.append(solver.current(seq[k]))
-            solver.observables()  # G_less_obs, dosd, trU, trD back to host buffers
+            J = solver.current(seq[k])
+            o = solver.observables()  # G_less_obs, dosd, trU, trD back to host buffers
+            points.append(dict(V=seq[k], converged=r["converged"], n_iter=r["n_iter"], n_mixed=r["n_mixed"],
+                               seconds=r["seconds"], J=J, occ=np.imag(np.diag(o["G_less_obs"])).copy(),
+                               G=o["G_less_obs"], dosd=o["dosd"]))
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
-        out = dict(launches=qb.kernel_launches() - l0, prof=solver.profile(False), clk=clocks.stop(), iters=iters,
-                   mixed_steps=mixed_steps, currents=currents, nA=solver.nA, Nf=solver.Nf, n_vec=solver.n_vec)
+        n_conv = sum(int(p["converged"]) for p in points)
+        out = dict(launches=qb.kernel_launches() - l0, prof=solver.profile(False), clk=clocks.stop(), points=points,
+                   nA=solver.nA, Nf=solver.Nf, n_vec=solver.n_vec)
         solver.close()
         if world > 1:
             dev_s, wall, n_conv = reduce_replicas(dev_s, wall, n_conv, device="cuda")
@@ -435,10 +537,9 @@ def main():
     head = arms.get("mixed") or arms["fp64"]
     f64 = arms.get("fp64")
     dev_s, wall, n_conv = head["dev_s"], head["wall"], head["n_conv"]
-    launches, clk, iters = head["launches"], head["clk"], head["iters"]
+    launches, clk = head["launches"], head["clk"]
     prof = (f64 or head)["prof"]
     if rank == 0:
-        points = args.steps * world
         peaks, src = measured_peaks()
         # roofline of the dominant kernel of the FP64 form (largest device time):
         # algorithmic work per launch
@@ -454,12 +555,12 @@ def main():
             "sig2_invC": ("hbm", 2.0 * nA * nA * Nf * 16.0 + 2.0 * nA * nA * n * 16.0),  # read V, write Sigma
             "broyden": ("hbm", nvec * (64.0 + 12.0 * nh) / 3.0),          # per iteration / 3 launches
         }
-        # DRAM bytes per energy measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on
-        # the 120x120 helix with 1024 energies (profiles/dyson_bgj_helix120_n1024.md,
-        # profiles/keldysh_tc_helix120_n1024.md); the traffic of a launch is per energy, so it
-        # scales with the number of energies
-        traffic_per_energy = {"dyson_gj": (236.776192e6 + 183.729152e6) / 1024,
-                              "keldysh_scf2": (1064.643e6 + 800.101376e6) / 1024}
+        # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+        # on the 120x120 helix: Dyson and Keldysh per energy at 1024 energies
+        # (profiles/dyson_bgj_helix120_n1024.md, profiles/keldysh_tc_helix120_n1024.md); the
+        # Broyden kernels per vector element (profiles/broyden_kernels_helix120.md)
+        traffic_per_unit = {"dyson_gj": ((236.776192e6 + 183.729152e6) / 1024, n),
+                            "keldysh_scf2": ((1064.643e6 + 800.101376e6) / 1024, n)}
         roof = None
         if fam in work and cnt:
             kind, per_launch = work[fam]
@@ -470,42 +571,45 @@ def main():
             else:
                 achieved, peak, unit = per_launch / t / 1e9, peaks.get("hbm_gbs", 6650.0), "GB/s"
                 src_note = f"hbm_gbs of MEASURED_PEAKS.json ({src})"
-            tpe = traffic_per_energy.get(fam) if (N, nA) == (120, 120) else None
+            tpu = traffic_per_unit.get(fam) if (N, nA) == (120, 120) else None
             roof = {"kernel": fam, "bound": kind, "achieved": achieved, "peak": peak, "unit": unit,
-                    "frac": achieved / peak, "traffic": tpe * n if tpe else None,
-                    "traffic_note": "DRAM bytes per launch, ncu capture at 1024 energies scaled to the launch" if tpe else None,
+                    "frac": achieved / peak, "traffic": tpu[0] * tpu[1] if tpu else None,
+                    "traffic_note": "DRAM bytes per launch from an ncu capture, scaled per unit" if tpu else None,
                     "peak_source": src_note,
                     "per_launch_work": per_launch, "launches": cnt, "avg_launch_ms": ms / cnt}
         prec_name = "mixed" if "mixed" in arms else "fp64"
+        pts = head["points"]
         line = {
             "metric": "converged IV points/s", "value": n_conv / dev_s if dev_s > 0 else 0.0,
             "unit": "IV points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if prec_name == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": f"helix {ions}x{turns} ({N}x{N} complex), {n} energies on [-12,12] eV, order 2, U=1.0 eV, "
-                                   "V sweep -1..1 V step 0.05 with continuation", "precision": prec_name, "nhist": args.nhist,
-                       "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 (no flush needed)",
-                       "scf_steps_per_point": iters, "converged_points": n_conv},
+            "config": bench_config(n, ions, turns, args.nhist, world),
+            "form": prec_name,
+            "voltages": [p["V"] for p in pts],
+            "converged": [bool(p["converged"]) for p in pts],
+            "scf_steps_per_point": [p["n_iter"] for p in pts],
+            "converged_points": n_conv,
             "e2e": {"value": n_conv / wall if wall > 0 else 0.0, "unit": "IV points/s", "h2d_bytes_per_step": 8,
                     "d2h_bytes_per_step": obs_bytes},
             "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]},
             "roofline": roof,
             "clocks": clk,
-            "currents_A": [list(c) for c in head["currents"]],
+            "currents_A": [list(p["J"]) for p in pts],
         }
         if "mixed" in arms:
-            line["config"]["mixed"] = ("Sigma2 FFTs, 2x2 algebra and spectra in FP32 while max|F| > max(1e-5, 100 tolf) "
-                                       "(the FP32 noise floor is ~1e-5); then FP64 steps until an FP64 residual meets "
-                                       "tolf; Dyson/Keldysh, Broyden and observables FP64")
-            line["config"]["fp32_steps_per_point"] = head["mixed_steps"]
+            line["mixed_form"] = ("Sigma2 FFTs, 2x2 algebra and spectra in FP32 while max|F| > max(1e-5, 100 tolf) "
+                                  "(the FP32 noise floor is ~1e-5); then FP64 steps until an FP64 residual meets "
+                                  "tolf; Dyson/Keldysh, Broyden and observables FP64")
+            line["fp32_steps_per_point"] = [p["n_mixed"] for p in pts]
         if f64 is not None and "mixed" in arms:
-            j64, jmx = np.array(f64["currents"]), np.array(head["currents"])
             line["fp64"] = {"value": f64["value"], "e2e": f64["e2e"], "ms_per_step": 1000.0 * f64["dev_s"] / args.steps,
-                            "scf_steps_per_point": f64["iters"], "kernel_ms": {k: round(v[0], 3) for k, v in
-                                                                               f64["prof"].items() if v[1]}}
+                            "converged": [bool(p["converged"]) for p in f64["points"]],
+                            "scf_steps_per_point": [p["n_iter"] for p in f64["points"]],
+                            "kernel_ms": {k: round(v[0], 3) for k, v in f64["prof"].items() if v[1]}}
             line["mixed_over_fp64"] = head["value"] / f64["value"] if f64["value"] > 0 else None
-            line["current_rel_err_vs_fp64"] = float(np.max(np.abs(jmx - j64)) / np.max(np.abs(j64)))
+            line["err_vs_fp64"] = observable_errors(f64["points"], pts)
             line["kernel_ms_mixed"] = {k: round(v[0], 3) for k, v in head["prof"].items() if v[1]}
         if world == 1 and args.serve > 0:
             line["serving"] = run_serving(qb, args.serve, args.serve_rate, args.serve_inflight, qb.QS_PREC_FP64)
@@ -516,7 +620,8 @@ def main():
         if world == 1:
             line["setup"] = setup_timing(qb, m)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_sample(args.ref_sample)
+            line["cpu_baseline"] = cpu_baseline_line(qb, seq[args.warmup:args.warmup + args.cpu_points], args.ref_sample,
+                                                     ions, turns, local)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

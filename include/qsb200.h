@@ -4,8 +4,9 @@
  *
  * The reference calls these steps from Fortran module procedures; each entry point below
  * names the reference interface it replaces (file:line, paths relative to the reference
- * project). A Fortran caller binds them with ISO_C_BINDING; the
- * argument layout is the one the reference already uses:
+ * project). A Fortran caller binds them with ISO_C_BINDING (an interface block of
+ * bind(C) procedures with value/reference arguments as declared here); the argument
+ * layout is the one the reference already uses:
  *   - matrices column-major, complex(dp) = two doubles (re, im);
  *   - packed SCF vectors in the layout of pack_gf (common/linear_algebra.f90:155-191)
  *     or pack_nil (src/scf.f90:226-240);
@@ -100,7 +101,9 @@ int qs_fft_length(const qs_handle *h);
  * G^<(t=0) + pack_nil (src/scf.f90:103-110) at order 1: the fresh-start SCF vector. */
 int qs_initial_vector(qs_handle *h, double Volt, double *x);
 
-/* scf_residual2 / scf_residual1 (src/scf.f90:158-224): F = pack(G_out[x]) - x. */
+/* scf_residual2 / scf_residual1 (src/scf.f90:158-224): F = pack(G_out[x]) - x. On a
+ * QS_PREC_MIXED handle the order-2 residual is evaluated as in the FP32 phase of its solves
+ * (FP32 self-energies; Keldysh products on the tensor cores in 3xTF32 for 32 <= nA <= 128). */
 int qs_residual(qs_handle *h, double Volt, const double *x, double *F, int *abort_flag);
 
 /* unpack_gf + equal_time_lesser + sigma_first_order + sigma2_compute(.true.)
@@ -165,9 +168,9 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
  * replaced by their inverses; info[b] = 0, or k+1 for a zero pivot at step k. The work
  * runs asynchronously on `stream` (a cudaStream_t, NULL = legacy default stream); read info
  * after synchronising. The library allocates nothing: its workspace is a fixed 16 MiB
- * device array that every GPU loading the library holds until exit. The first call on
- * each device looks up that array's address (cudaGetSymbolAddress) with the device
- * current; make this first call before any stream capture. All calls share the array, so
+ * device array that every GPU loading the library holds until exit. Each call looks up
+ * that array's address (cudaGetSymbolAddress) on the calling thread's current device; the
+ * first call on a device may load the module there, so make it before any stream capture. All calls share the array, so
  * calls that overlap on the GPU (other streams or threads) race: serialise them. Limits:
  * 1 <= N <= 512 (else QS_ERR_NOALLOC_LIMIT, with a message on stderr). Returns 0 or a
  * CUDA error (< 0). */

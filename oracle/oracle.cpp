@@ -75,6 +75,11 @@ struct FFTPlan {
     int n = 0;
     std::vector<int> radix;
     std::vector<cplx> tw;  // tw[k] = exp(-2 pi i k / n)
+    // power-of-two lengths: radix-4 Stockham stages (one radix-2 stage first when log2 n
+    // is odd), stage s with span L holding the twiddles w^(j*n/(4L)), j < L, contiguously
+    bool pow2 = false;
+    std::vector<int> p2_span;             // L of each radix-4 stage
+    std::vector<std::vector<cplx>> p2_tw;  // per stage: [w1, w2, w3] for j = 0..L-1
     void init(int nn) {
         n = nn;
         radix.clear();
@@ -86,6 +91,59 @@ struct FFTPlan {
             long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)n;
             tw[k] = cplx((double)cosl(a), (double)sinl(a));
         }
+        pow2 = n >= 4 && (n & (n - 1)) == 0;
+        p2_span.clear();
+        p2_tw.clear();
+        if (pow2) {
+            int L = ((__builtin_ctz(n) & 1) ? 2 : 1);
+            for (; L < n; L *= 4) {
+                std::vector<cplx> t(3 * (size_t)L);
+                const int step = n / (4 * L);
+                for (int j = 0; j < L; j++)
+                    for (int q = 1; q <= 3; q++) t[3 * (size_t)j + q - 1] = tw[(size_t)q * j * step];
+                p2_span.push_back(L);
+                p2_tw.push_back(std::move(t));
+            }
+        }
+    }
+    // power-of-two transform: Stockham autosort, out of place between x and work
+    void exec_pow2(cplx *x, cplx *work, int sign) const {
+        cplx *a = x, *b = work;
+        int L = 1;
+        if (__builtin_ctz(n) & 1) {  // radix-2 stage: b[2j + {0,1}] from a[j], a[j + n/2]
+            const int h = n / 2;
+            for (int j = 0; j < h; j++) {
+                cplx u = a[j], v = a[j + h];
+                b[2 * j] = u + v;
+                b[2 * j + 1] = u - v;
+            }
+            std::swap(a, b);
+            L = 2;
+        }
+        // stage with span L: input a viewed as [4][n/4] blocks of sub-transforms of length L
+        // (element (r, k*L + j)), output b as sub-transforms of length 4L (k*4L + q*L + j)
+        for (size_t s = 0; s < p2_span.size(); s++) {
+            L = p2_span[s];
+            const cplx *t = p2_tw[s].data();
+            const int m4 = n / 4, K = m4 / L;
+            for (int k = 0; k < K; k++)
+                for (int j = 0; j < L; j++) {
+                    cplx w1 = t[3 * j], w2 = t[3 * j + 1], w3 = t[3 * j + 2];
+                    if (sign > 0) { w1 = std::conj(w1); w2 = std::conj(w2); w3 = std::conj(w3); }
+                    const int i0 = k * L + j;
+                    cplx v0 = a[i0], v1 = a[i0 + m4] * w1, v2 = a[i0 + 2 * m4] * w2, v3 = a[i0 + 3 * m4] * w3;
+                    cplx s02 = v0 + v2, d02 = v0 - v2, s13 = v1 + v3, d13 = v1 - v3;
+                    // multiply d13 by -i (forward) or +i (backward)
+                    cplx rd13 = sign < 0 ? cplx(d13.imag(), -d13.real()) : cplx(-d13.imag(), d13.real());
+                    cplx *o = b + (size_t)k * 4 * L + j;
+                    o[0] = s02 + s13;
+                    o[L] = d02 + rd13;
+                    o[2 * L] = s02 - s13;
+                    o[3 * L] = d02 - rd13;
+                }
+            std::swap(a, b);
+        }
+        if (a != x) std::memcpy(x, a, sizeof(cplx) * n);
     }
     cplx w(long k, int sign) const {  // exp(sign * 2 pi i k / n)
         long kk = ((k % n) + n) % n;
@@ -93,6 +151,10 @@ struct FFTPlan {
     }
     // in-place transform of x (length n); work has length n
     void exec(cplx *x, cplx *work, int sign) const {
+        if (pow2) {
+            exec_pow2(x, work, sign);
+            return;
+        }
         cplx *a = x, *b = work;
         int Ns = 1;
         cplx v[8], o[8];

@@ -284,13 +284,16 @@ __global__ void part_reduce(const double *__restrict__ part, int nb, int stride,
 }
 
 // Cholesky solve of the nh x nh system (w0^2 I + dF^T dF) gamma = dF^T F, as dposv('U').
-// Returns 0 or the LAPACK-style info (> 0: not positive definite).
+// Returns 0 or the LAPACK-style info (> 0: not positive definite). A pivot fails only when
+// it is <= 0, as in the OpenBLAS dpotrf the reference links (its unblocked factorisation
+// tests ajj <= 0): a NaN pivot passes and the NaN reaches gamma, so a non-finite Gram matrix
+// does not reset the history there either.
 static int chol_solve(int nh, const std::vector<double> &A0, int lda, std::vector<double> &b) {
     std::vector<double> U((size_t)nh * nh, 0.0);
     for (int j = 0; j < nh; j++) {
         double s = A0[j + (size_t)j * lda];
         for (int k = 0; k < j; k++) s -= U[k + (size_t)j * nh] * U[k + (size_t)j * nh];
-        if (!(s > 0.0)) return j + 1;
+        if (s <= 0.0) return j + 1;
         double ujj = std::sqrt(s);
         U[j + (size_t)j * nh] = ujj;
         for (int i = j + 1; i < nh; i++) {
@@ -357,7 +360,7 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
             break;
         }
         // history pair, Gram column, dF^T F
-        bool store = want_dn && fnorm > 0.0;
+        bool store = want_dn && fnorm > 0.0 && !res.precision_changed();
         int slot = want_dn ? nstored % nhist : 0;
         int nh_new = store ? std::min(nstored + 1, nhist) : std::min(nstored, nhist);
         if (nh_new > 0 || store) {

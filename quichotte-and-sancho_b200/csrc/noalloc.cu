@@ -11,11 +11,12 @@
 // global workspace that qs_create / qs_invert_batched allocate. Here the workspace is the
 // file-scope array below instead: QS_NOALLOC_SCRATCH_BYTES (16 MiB) on every GPU that loads
 // this library, held until the process exits. Every matrix goes through it, whatever N.
-// Its device address is looked up once per device (cudaGetSymbolAddress, on the first call
-// made on that device with the device current); host code never uses the symbol itself.
+// Its device address is looked up on every call (cudaGetSymbolAddress with the caller's
+// device current), so a context that was destroyed and created again (cudaDeviceReset)
+// never leaves a stale address behind; host code never uses the symbol itself. The first
+// call on a device may load the module there, so it should come before any stream capture.
 #include <climits>
 #include <cstdio>
-#include <mutex>
 
 #include "qs_common.cuh"
 
@@ -24,27 +25,16 @@ namespace {
 constexpr size_t QS_NOALLOC_SCRATCH_BYTES = 16u << 20;  // 16 MiB
 constexpr size_t QS_NOALLOC_HEADER = 256;               // first bytes: the min-info word
 constexpr int QS_NOALLOC_MAX_N = 512;                   // the kernel's limit (>= 3 slots of 512^2 fit)
-constexpr int QS_MAX_DEVICES = 128;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[QS_NOALLOC_SCRATCH_BYTES];
 
-std::mutex g_mu;
-void *g_scratch_addr[QS_MAX_DEVICES] = {nullptr};
-
-// device address of the scratch array on the current device (set up once per device)
+// device address of the scratch array in the current context of the current device
 int scratch_address(void **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return -(int)e;
-    if (dev < 0 || dev >= QS_MAX_DEVICES) return -1;
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) return e != cudaSuccess ? -(int)e : -1;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    if (p == nullptr) return -1;
+    *out = p;
     return 0;
 }
 

@@ -225,6 +225,32 @@ void count_launch();
 int prof_begin(qs_handle *h, int fam);
 void prof_end(qs_handle *h, int idx);
 
+__device__ __forceinline__ double fermi_d(double w, double V, double mu, double beta) {
+    // src/green_functions.f90:74-84 (hbar = 1)
+    double arg = (w - mu + V) * beta;
+    return 1.0 / (exp(fmin(arg, 700.0)) + 1.0);
+}
+
+// arguments of the Keldysh kernels (sweep modes M_INIT2 / M_SCF2)
+struct KeldyshArgs {
+    int nA, n;
+    int64_t nblk;
+    const zc *G;     // G_AA per energy (nA^2 complex)
+    const zc *SigL;  // Sigma2^< per energy, or nullptr
+    const zc *GamLs, *GamRs;
+    const double *omega;
+    double V, mu, beta;
+    double *out;        // DL blocks (SCF vector)
+    const double *xsub; // subtracted (F = out - x), or nullptr
+    zc *gRd, *gLd;      // diagonals, or nullptr
+    zc *Tws;            // per-block scratch, nA^2 complex
+    int *err;           // set to 1 if a bounded tensor-core wait gave up (tcgen05 kernel)
+};
+// the FP32-phase Keldysh step of a QS_PREC_MIXED solve on the fifth-generation tensor cores
+// (keldysh_tf32.cu): 32 <= nA <= 128; returns -1 for other sizes
+int launch_keldysh_tf32(qs_handle *h, const KeldyshArgs &k);
+bool keldysh_tf32_fits(int nA);
+
 // launchers (implemented in the .cu files)
 int sigma2_setup(qs_handle *h);
 // fp32: FFTs, 2x2 algebra and spectra in FP32 (QS_PREC_MIXED handles), Sigma written in FP64
@@ -250,7 +276,8 @@ int tune_launch(qs_handle *h, int kind, int size, const int *cand, int ncand, in
 int vec_maxabs(qs_handle *h, const double *d_v, int64_t n, double &mx);
 int equal_time_lesser_sigma1(qs_handle *h, const double *d_x);
 enum SweepMode { M_INIT2 = 1, M_SCF2 = 2, M_SCF1 = 3, M_FINAL = 4 };
-int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x);
+// fp32: the FP32 phase of a QS_PREC_MIXED solve (M_SCF2 only: tensor-core Keldysh products)
+int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x, bool fp32 = false);
 int sum_over_energies(qs_handle *h, const zc *d_A, int64_t ld, int ncols, int64_t nrows, zc *d_out);
 int sum_over_energies_real(qs_handle *h, const double *d_A, int64_t ld, int ncols, int64_t nrows, double *d_out);
 int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, zc *d_ws, int ws_slots);
@@ -263,6 +290,9 @@ int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, dou
 // that fills F (device) from x (device) and may set abort.
 struct BroydenResidual {
     virtual int operator()(const double *d_x, double *d_F, bool &abort) = 0;
+    // true if the residual just evaluated used another precision than the one before: the
+    // (dF, u) pair of this step would mix two different residual functions and is not stored
+    virtual bool precision_changed() const { return false; }
     virtual ~BroydenResidual() = default;
 };
 struct BroydenOut {

@@ -175,8 +175,17 @@ SanityOut check_diag_sanity(int nb, const std::vector<zc> &sumL, const std::vect
 }
 
 int read_info(qs_handle *h, int &info) {
-    QS_CUDA(h, cudaMemcpyAsync(&info, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    int hv[2];
+    QS_CUDA(h, cudaMemcpyAsync(hv, h->d_info, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     QS_CUDA(h, cudaStreamSynchronize(h->stream));
+    info = hv[0];
+    if (hv[1] != 0) {  // a bounded tensor-core wait gave up (the kernel freed its TMEM and returned)
+        h->err = "tensor-core Keldysh kernel: an mbarrier wait timed out";
+        int z = 0;
+        QS_CUDA(h, cudaMemcpyAsync(h->d_info + 1, &z, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+        QS_CUDA(h, cudaStreamSynchronize(h->stream));
+        return -3;
+    }
     if (info != INT_MAX) {
         h->err = "ERROR: ZGETRF failed (singular matrix?) at energy index " + std::to_string(info);
         int v = INT_MAX;
@@ -276,13 +285,15 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 }
 
 // The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: the leading steps form the
-// second-order self-energies in FP32 (FFTs, 2x2 algebra and spectra); once max|F| falls
-// below mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the solve
+// second-order self-energies in FP32 (FFTs, 2x2 algebra and spectra) and the Keldysh
+// products on the tensor cores (3xTF32, keldysh_tf32.cu); once max|F| falls below
+// mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the solve
 // continues in FP64 (an FP32 step whose max|F| is already below tolf is redone in FP64
 // first, so that it cannot end the solve). The FP32 self-energies leave a noise floor of
 // about 1e-5 in F on the 120x120 helix, so FP32 steps stop well above it. Convergence
 // (max|F| < tolf) is always decided on an FP64 residual, and the converged state meets the
-// FP64 solve's criterion.
+// FP64 solve's criterion. The Broyden pair of the first FP64 step (its dF is an FP64
+// residual minus an FP32 one) is not stored (precision_changed).
 struct Residual2 : BroydenResidual {
     qs_handle *h;
     double V;
@@ -291,11 +302,13 @@ struct Residual2 : BroydenResidual {
     int n_mixed = 0;
     double best = HUGE_VAL;
     int since_best = 0;
+    int last_prec = -1, cur_prec = -1;  // 1 = FP32 phase, 0 = FP64, of the last two evaluations
+    bool precision_changed() const override { return last_prec >= 0 && last_prec != cur_prec; }
     int eval(const double *d_x, double *d_F, bool &abort, bool use32) {
         int rc;
         if ((rc = equal_time_lesser_sigma1(h, d_x))) return rc;
         if ((rc = sigma2_compute(h, d_x, use32))) return rc;
-        if ((rc = sweep(h, M_SCF2, V, true, d_F, d_x))) return rc;
+        if ((rc = sweep(h, M_SCF2, V, true, d_F, d_x, use32))) return rc;
         SanityOut s;
         if ((rc = sweep_sanity(h, s))) return rc;
         abort = s.runaway;
@@ -304,6 +317,8 @@ struct Residual2 : BroydenResidual {
     }
     int operator()(const double *d_x, double *d_F, bool &abort) override {
         iter++;
+        last_prec = cur_prec;
+        cur_prec = fp32 ? 1 : 0;
         int rc;
         if (!fp32) return eval(d_x, d_F, abort, false);
         if ((rc = eval(d_x, d_F, abort, true))) return rc;
@@ -321,6 +336,7 @@ struct Residual2 : BroydenResidual {
             fp32 = false;  // the next steps are FP64
             if (fmax < h->tolf) {  // never let an FP32 residual declare convergence: redo it
                 n_mixed--;
+                cur_prec = 0;
                 return eval(d_x, d_F, abort, false);
             }
         }
@@ -864,7 +880,8 @@ int qs_residual(qs_handle *h, double Volt, const double *x, double *F, int *abor
         Residual2 r;
         r.h = h;
         r.V = Volt;
-        if ((rc = r(h->d_x, h->d_Fold, ab))) return rc;
+        // a QS_PREC_MIXED handle evaluates the residual of its solves' FP32 phase
+        if ((rc = r.eval(h->d_x, h->d_Fold, ab, h->precision == QS_PREC_MIXED))) return rc;
         if ((rc = convert_dl_to_ref(h->stream, h->nA, h->n, h->d_Fold, h->d_F))) return -rc;
         QS_CUDA(h, cudaMemcpyAsync(F, h->d_F, sizeof(double) * h->n_vec, cudaMemcpyDeviceToHost, h->stream));
         QS_CUDA(h, cudaStreamSynchronize(h->stream));

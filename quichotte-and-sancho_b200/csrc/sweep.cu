@@ -19,11 +19,6 @@
 
 namespace qs {
 
-__device__ __forceinline__ double fermi_d(double w, double V, double mu, double beta) {
-    // src/green_functions.f90:74-84 (hbar = 1)
-    double arg = (w - mu + V) * beta;
-    return 1.0 / (exp(fmin(arg, 700.0)) + 1.0);
-}
 
 // ---------------------------------------------------------------------------------
 // Block-wide argmax of cabs1 over rows k..N-1 of column k (first maximum wins, as
@@ -529,20 +524,6 @@ __device__ void cta_gemm(int M, int N, int K, LA la, LB lb, ST st, zc *sA, zc *s
             }
     }
 }
-
-struct KeldyshArgs {
-    int nA, n;
-    int64_t nblk;
-    const zc *G;     // G_AA per energy (nA^2 complex)
-    const zc *SigL;  // Sigma2^< per energy, or nullptr
-    const zc *GamLs, *GamRs;
-    const double *omega;
-    double V, mu, beta;
-    double *out;        // DL blocks (SCF vector)
-    const double *xsub; // subtracted (F = out - x), or nullptr
-    zc *gRd, *gLd;      // diagonals, or nullptr
-    zc *Tws;            // per-block scratch, nA^2 complex
-};
 
 // modes M_INIT2 / M_SCF2: T = G^r SL, G^< = T G^r^dagger (upper triangle), packed.
 __global__ void __launch_bounds__(256) keldysh_scf2(KeldyshArgs a) {
@@ -1172,7 +1153,7 @@ int invert_batched_ws(cudaStream_t st, int N, int batch, zc *d_A, int *d_min_inf
 // sweep(mode) over all energies (src/scf.f90:280-290).
 //   M_INIT2 / M_SCF2: output into d_out (SCF vector, DL); M_SCF2 subtracts d_x.
 //   M_SCF1 / M_FINAL: per-energy arrays of the handle.
-int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x) {
+int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const double *d_x, bool fp32) {
     const int N = h->Norb, nA = h->nA, n = h->n;
     DysonArgs a{};
     a.N = N;
@@ -1216,6 +1197,9 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gRd = h->d_gRd;
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
+        k.err = h->d_info + 1;
+        // the FP32 phase of a QS_PREC_MIXED solve: G^< on the fifth-generation tensor cores
+        if (fp32 && mode == M_SCF2 && keldysh_tf32_fits(nA)) return launch_keldysh_tf32(h, k);
         const int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
         const int nbt = std::min(n, 148);
         auto launch_k = [&](int v) -> int {

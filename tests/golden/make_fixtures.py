@@ -2,7 +2,7 @@
 container that has the reference checked out; the copies are committed so the GPU
 tests can use them where the reference is absent).
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py /path/to/reference
 
 Copied: tests/cases.txt and every tests/cases/<case>/ (inputs such as input.dat,
 DFTB+ matrices, xyz and U files, and the golden outputs under reference/). These files
@@ -28,4 +28,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py /path/to/reference")
+    main(sys.argv[1])

@@ -216,6 +216,27 @@ def test_mixed_sigma2_within_fp32_tolerance_of_oracle(delta):
     assert rel(SRg, SRo) > 1e-12  # the FP32 path ran
 
 
+@pytest.mark.parametrize("ions_turns", LARGE_HELICES)
+def test_mixed_residual_tensor_core_keldysh_matches_oracle(ions_turns):
+    """The FP32-phase residual of a mixed handle (FP32 Sigma2, Keldysh products on the
+    fifth-generation tensor cores in 3xTF32 with FP32 accumulation, nA = 56, 100, 120):
+    F within 2e-5 of the FP64 oracle relative to the largest |G_out| element, the G^r part
+    exact to FP64 rounding of the Dyson inputs' FP32 self-energies, and clearly not the FP64
+    path (the difference is above FP64 rounding)."""
+    ni, nt = ions_turns
+    m = qb.Model.helix(N_ions=ni, N_turns=nt, hel_length=0.34 * nt, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                       lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
+                       dw=1.0, up=1.0, delta=0.04, order=2)
+    gs, os_ = qb.Solver(m, precision=qb.QS_PREC_MIXED), oracle_lib.solver(m)
+    x = os_.initial_vector(0.2) + 1e-3 * np.random.default_rng(6).standard_normal(gs.n_vec)
+    Fg, ag = gs.residual(0.2, x)
+    Fo, ao = os_.residual(0.2, x)
+    assert not ag and not ao
+    scale = np.max(np.abs(Fo + x))
+    err = np.max(np.abs(Fg - Fo)) / scale
+    assert 1e-12 < err < 2e-5, err
+
+
 @pytest.mark.parametrize("case", ORDER2)
 def test_mixed_solve_matches_fp64_solve(case):
     """A mixed solve converges on FP64 residuals: currents, occupations and the spectral

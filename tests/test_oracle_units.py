@@ -20,7 +20,7 @@ def good_fft_size(nmin):
         n += 1
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 7, 8, 12, 21, 60, 105, 672, 720, 1000, 4096, 8192])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 7, 8, 12, 16, 21, 32, 60, 105, 672, 720, 1000, 2048, 4096, 8192, 32768])
 @pytest.mark.parametrize("sign", [-1, 1])
 def test_oracle_fft_matches_numpy(n, sign):
     lib = oracle_lib.lib()
