@@ -111,6 +111,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def finite(obj):
+    """The line's values with every non-finite float replaced by None (strict JSON)."""
+    if isinstance(obj, dict):
+        return {k: finite(v) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [finite(v) for v in obj]
+    if isinstance(obj, (float, np.floating)):
+        return float(obj) if np.isfinite(obj) else None
+    if isinstance(obj, np.integer):
+        return int(obj)
+    return obj
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -121,8 +134,17 @@ def measured_peaks():
 # Broyden settings of the workload: the reference's input defaults (src/input_output.f90:
 # 109-114). Both arms and every form use them.
 BROYDEN = dict(alpha_mix=0.5, nhist=16, tolf=1e-6, maxscf=300, single_history=1)
-# energies of the CPU sample grid (the same helix and window; see cpu_sample_sweep)
-SAMPLE_N = 512
+# energies of the CPU sample: 1/16 of the grid (every part of an SCF iteration, residual
+# and Broyden update, does the same work per energy)
+SAMPLE_N = 1024
+# SCF iterations per voltage of this sweep in the FP64 form on B200 (all 41 voltages, swept
+# -1 -> 1 V with continuation, fresh after an unconverged voltage, maxscf 300; one B200, the
+# default Broyden settings); 300 marks a voltage that did not converge. The CPU arm multiplies
+# its measured time per iteration by this work (the oracle runs the same algorithm, so the same
+# iterations).
+SWEEP_ITERS_B200 = dict(zip(VOLTS, [32, 27, 27, 26, 25, 25, 24, 23, 22, 21, 20, 19, 18, 16, 19, 18, 24, 24, 228,
+                                    300, 300, 300, 300, 300, 300, 300, 210, 16, 18, 20, 23, 25, 26, 27, 28, 27,
+                                    28, 29, 30, 30, 31]))
 
 
 def bench_config(n_omega, ions, turns, nhist, world):
@@ -138,74 +160,198 @@ def bench_config(n_omega, ions, turns, nhist, world):
             "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 126 MB (no flush needed)"}
 
 
-def cpu_sample_sweep(volts, n_sample=SAMPLE_N, threads=None, ions=N_IONS, turns=N_TURNS):
-    """The CPU oracle (oracle/oracle_py.py: the model built in numpy, only liboracle.so loaded)
-    on a bounded sample of the sweep: real converged IV points of the same helix, physics,
-    window and Broyden settings at the voltages `volts` (continuation from the first, fresh
-    after an unconverged point, as src/quichotte.f90:125-143), on a grid of n_sample energies
-    instead of 16384. Returns per-point wall times, step counts and currents."""
+def _oracle(threads):
     if threads:
         os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
-    m = oracle_py.Helix(ions, turns, PITCH * turns * (ions - 1) / ions, RADIUS, 1.0, 0.0, 1.0, 0.01, 1.0, 0.5, 0.5,
-                        0.5, 300.0, 0.0, W_LO, (W_HI - W_LO) / n_sample, n_sample)
-    s = oracle_py.Solver(m, **BROYDEN)
+    return oracle_py
+
+
+def cpu_iteration_times(V, n_keep, n_sample=SAMPLE_N, threads=None, ions=N_IONS, turns=N_TURNS):
+    """Wall times of n_keep SCF iterations of the CPU oracle (oracle/oracle_py.py: the model
+    built in numpy, only liboracle.so loaded) on the same helix, window and Broyden settings
+    with n_sample energies, counting only iterations with a full history (the steady state
+    of a solve); tolf = 0, so every iteration does its whole work."""
+    op = _oracle(threads)
+    m = op.Helix(ions, turns, PITCH * turns * (ions - 1) / ions, RADIUS, 1.0, 0.0, 1.0, 0.01, 1.0, 0.5, 0.5, 0.5, 300.0,
+                 0.0, W_LO, (W_HI - W_LO) / n_sample, n_sample)
+    nh_full, times = BROYDEN["nhist"], []
+    for _ in range(4):  # a solve that runs away ends early: start again
+        s = op.Solver(m, **dict(BROYDEN, tolf=0.0, maxscf=nh_full + 3 + n_keep - len(times)))
+        r, dt = s.solve_timed(V, True)
+        s.close()
+        times += [t for t, step in zip(dt, r["log"]) if step[3] == nh_full]
+        if len(times) >= n_keep:
+            break
+    return times[:n_keep]
+
+
+def iters_per_converged_point(volts, iters, converged):
+    """SCF iterations the sweep spent per converged IV point over `volts`."""
+    it = sum(iters[V] for V in volts)
+    conv = sum(int(converged[V]) for V in volts)
+    return it / conv if conv else 0.0
+
+
+def model_cfg0(qb, n_omega=4096):
+    """The CPU-runnable configuration: 4 sites/turn x 2 turns (16 x 16 H), U = 0.5 eV, 4096
+    energies on [-10, 10] eV, Broyden mixing 0.1 and tolf 1e-8 (reference history otherwise)."""
+    args = dict(N_ions=4, N_turns=2, hel_length=PITCH * 2 * 3 / 4, hel_radius=RADIUS, hand=1.0, E_CC=0.0, t_hop=1.0,
+                lamb=0.01, U_int=0.5, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0)
+    ev = np.linalg.eigvalsh(qb.Model.helix(dw=1.0, up=1.0, delta=0.1, **args).H)
+    delta = 20.0 / n_omega
+    m = qb.Model.helix(dw=ev[0] + 10.0, up=10.0 - ev[-1] + 0.5 * delta, delta=delta, **args)
+    assert m.n_omega == n_omega, m.n_omega
+    return m
+
+
+HARTREE = 27.211386245988  # eV; the DFTB+ files hold H0 in Hartree (src/hamiltonian.f90:612)
+
+
+def _dftb_square(path, A):
+    """A DFTB+ square matrix file as read by read_dftb_square (src/hamiltonian.f90:556-609)."""
+    n = A.shape[0]
+    with open(path, "w") as f:
+        f.write(f"#      REAL   NALLORB   NKPOINT\n          T {n:9d}         1\n#   IKPOINT\n          1\n# MATRIX\n")
+        for row in A:
+            f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
+
+
+def make_cfg2_case(path, n_omega=32768, seed=40):
+    """The synthetic helicene-like molecule of the multi-orbital configuration, written as a
+    dftb_hs case (hamiltonian = dftb_hs; seeded): 28 C (s, py, pz, px) on a helix of 6 atoms
+    a turn (radius 0.14 nm, 0.35 nm a turn) and 12 H (s) on every other C, 0.11 nm further out
+    (124 orbitals, 248 spin-orbitals). H0: on-site -6 eV (C s), 0 eV (C p), -2 eV (H s);
+    Slater-Koster-like hoppings -2.5 eV exp(-(r - 0.14 nm)/0.1 nm) times the direction cosines
+    of the p orbitals involved, within 0.45 nm, plus N(0, 0.05 eV) noise; written in Hartree.
+    S = I + P with P symmetric, ||P||_2 = 0.08 (so S is positive definite). p-shell SOC
+    xi = 0.00849 eV in the dual form. U = 0.8 eV on the 64 orbitals of C1..C15 and C28 (the two
+    contact atoms included, so the active block is 128 spin-orbitals), 0 elsewhere. Leads on
+    C1 (left) and C28 (right). The grid spans the spectrum +-1 eV with n_omega points."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(path, exist_ok=True)
+    nC, nH = 28, 12
+    th = 2 * np.pi * np.arange(nC) / 6
+    posC = np.stack([0.14 * np.cos(th), 0.14 * np.sin(th), 0.35 * np.arange(nC) / 6], axis=1)
+    hC = np.arange(0, 2 * nH, 2)  # C atoms carrying an H
+    posH = np.stack([0.25 * np.cos(th[hC]), 0.25 * np.sin(th[hC]), posC[hC, 2]], axis=1)
+    pos = np.vstack([posC, posH])
+    elem = ["C"] * nC + ["H"] * nH
+    orb = []  # (atom, kind) with kind 0 = s, 1..3 = py, pz, px
+    for a, e in enumerate(elem):
+        orb += [(a, 0)] + ([(a, 1), (a, 2), (a, 3)] if e == "C" else [])
+    No = len(orb)
+    H0 = np.zeros((No, No))
+    for i, (a, ka) in enumerate(orb):
+        H0[i, i] = (-6.0 if ka == 0 else 0.0) if elem[a] == "C" else -2.0
+    dirc = {1: 1, 2: 2, 3: 0}  # py, pz, px -> y, z, x
+    for i, (a, ka) in enumerate(orb):
+        for j, (b, kb) in enumerate(orb):
+            if j <= i or a == b:
+                continue
+            d = pos[b] - pos[a]
+            r = np.linalg.norm(d)
+            if r > 0.45:
+                continue
+            l = d / r
+            f = (1.0 if ka == 0 else l[dirc[ka]]) * (1.0 if kb == 0 else -l[dirc[kb]])
+            t = -2.5 * np.exp(-(r - 0.14) / 0.1) * f + rng.normal(0.0, 0.05)
+            H0[i, j] = H0[j, i] = t
+    P = rng.standard_normal((No, No))
+    P = P + P.T
+    S = np.eye(No) + 0.08 * P / np.linalg.norm(P, 2)
+    _dftb_square(os.path.join(path, "hamsqr1.dat"), H0 / HARTREE)
+    _dftb_square(os.path.join(path, "oversqr.dat"), S)
+    with open(os.path.join(path, "molecule.xyz"), "w") as f:
+        f.write(f"{len(elem)}\nsynthetic helicene-like molecule [Angstrom]\n")
+        for e, p in zip(elem, pos):
+            f.write(f"{e} {10 * p[0]:.8f} {10 * p[1]:.8f} {10 * p[2]:.8f}\n")
+    inter = set(range(15)) | {27}
+    with open(os.path.join(path, "U_per_orbital.dat"), "w") as f:
+        for a, _ in orb:
+            f.write(f"{0.8 if a in inter else 0.0}\n")
+
+    def write_input(dw, up, delta):
+        with open(os.path.join(path, "input.dat"), "w") as f:
+            f.write("hamiltonian = dftb_hs\nham_file = hamsqr1.dat\noverlap_file = oversqr.dat\n"
+                    "xyz_file = molecule.xyz\nmax_angular_momentum = C:p H:s\nsoc_xi = C:0.00849\n"
+                    "soc_form = dual\nlead_left_atoms = 1\nlead_right_atoms = 28\nhubbard_file = U_per_orbital.dat\n"
+                    f"T = 300.d0\nV = 0.1d0\nVf = 0.3d0\ndelv = 0.1d0\nmu = 0.0d0\norder = 2\nU_int = 0.8d0\n"
+                    f"GammaL_up = 0.5d0\nGammaL_down = 0.5d0\nGammaR = 0.5d0\ndw = {float(dw)!r}\n"
+                    f"up = {float(up)!r}\ndelta = {float(delta)!r}\n")
+    write_input(1.0, 1.0, 0.05)
+    return write_input
+
+
+def model_cfg2(qb, path, n_omega):
+    """The cfg2 case loaded through the host layer, its grid fitted to n_omega points."""
+    write_input = make_cfg2_case(path, n_omega)
+    ev = qb.Model.load(path).Ev
+    delta = (ev[-1] - ev[0] + 2.0) / n_omega
+    write_input(1.0, 1.0 + 0.5 * delta, delta)
+    m = qb.Model.load(path)
+    assert m.n_omega == n_omega, m.n_omega
+    return m
+
+
+CFG0_BROYDEN = dict(alpha_mix=0.1, nhist=16, tolf=1e-8, maxscf=300, single_history=1)
+CFG0_VOLTS = [round(0.1 * k, 10) for k in range(11)]
+
+
+def cfg0_sweep(solver):
+    """The cfg0 sweep V = 0..1 V step 0.1 with continuation: per-point converged flag,
+    iterations, currents, wall time of the sweep."""
     out, ok = [], False
-    for k, V in enumerate(volts):
-        r = s.solve_scf(V, k == 0 or not ok)
+    t0 = time.perf_counter()
+    for k, V in enumerate(CFG0_VOLTS):
+        r = solver.solve_scf(V, k == 0 or not ok)
         ok = r["converged"]
-        out.append(dict(V=V, converged=ok, n_iter=r["n_iter"], wall=r["wall"], J=s.current(V)))
-    s.close()
-    return out
+        out.append((ok, r["n_iter"], solver.current(V)))
+    return out, time.perf_counter() - t0
 
 
-def scaled_cpu_rate(points, n_sample):
-    """IV points/s of the 16384-energy workload from the sample: converged sample points per
-    second x n_sample/16384 (the Dyson, Keldysh and Broyden work per SCF step is linear in the
-    number of energies and the FFT's n log n only slightly more, so this favours the CPU)."""
-    t = sum(p["wall"] for p in points)
-    conv = sum(int(p["converged"]) for p in points)
-    rate = conv / t if t > 0 else 0.0
-    return rate * n_sample / N_OMEGA, rate, t, conv
-
-
-def cpu_baseline_line(qb, volts, n_sample, ions, turns, device):
-    """cpu_baseline of the GPU arm's line: the CPU oracle on a bounded sample (the first
-    timed voltages, on the sample grid), and the GPU's FP64 form on exactly the same sample
-    points in the same run (device time and wall time), so that the two are compared on
-    identical work as well as through the scaled figure."""
+def cpu_baseline_line(qb, V, n_keep, ions, turns, device, iters_per_point, ipp_note):
+    """cpu_baseline of the GPU arm's line: (1) the CPU oracle's time per SCF iteration on a
+    1/16 sample of this workload (as in the reference arm), times the SCF iterations per
+    converged IV point of this run's FP64 sweep; (2) real, unscaled converged IV points of the
+    CPU-runnable configuration (the 4 x 2 helix, 4096 energies, V = 0..1 V) on the CPU oracle
+    and on the GPU's FP64 form in the same run."""
     nthr = os.cpu_count()
-    pts = cpu_sample_sweep(volts, n_sample, threads=nthr, ions=ions, turns=turns)
-    v, v_sample, t, conv = scaled_cpu_rate(pts, n_sample)
-    ms = model_cfg1(qb, n_sample, ions, turns)
-    s = qb.Solver(ms, device=device, **BROYDEN)
-    gdev, gwall, gconv, giters, gJ, ok = 0.0, 0.0, 0, [], [], False
-    for k, V in enumerate(volts):
-        t0 = time.perf_counter()
-        r = s.solve_scf(V, k == 0 or not ok)
-        J = s.current(V)
-        s.observables()
-        gwall += time.perf_counter() - t0
-        ok = r["converged"]
-        gdev += r["seconds"]
-        gconv += int(ok)
-        giters.append(r["n_iter"])
-        gJ.append(J)
-    s.close()
-    jc = np.array([p["J"] for p in pts])
-    jg = np.array(gJ)
+    times = cpu_iteration_times(V, n_keep, SAMPLE_N, threads=nthr, ions=ions, turns=turns)
+    t_it = float(np.mean(times)) * N_OMEGA / SAMPLE_N
+    v = 1.0 / (t_it * iters_per_point) if times and iters_per_point > 0 else 0.0
+    op = _oracle(nthr)
+    mq = model_cfg0(qb)
+    mo = op.Helix(4, 2, PITCH * 2 * 3 / 4, RADIUS, 1.0, 0.0, 1.0, 0.01, 0.5, 0.5, 0.5, 0.5, 300.0, 0.0, mq.w_init,
+                  mq.delta, mq.n_omega)
+    so = op.Solver(mo, **CFG0_BROYDEN)
+    cpu_pts, cpu_s = cfg0_sweep(so)
+    so.close()
+    sg = qb.Solver(mq, device=device, **CFG0_BROYDEN)
+    gpu_pts, gpu_s = cfg0_sweep(sg)
+    sg.close()
+    jc = np.array([p[2] for p in cpu_pts])
+    jg = np.array([p[2] for p in gpu_pts])
+    both = [k for k in range(len(CFG0_VOLTS)) if cpu_pts[k][0] and gpu_pts[k][0]]
+    cc, gc = sum(int(p[0]) for p in cpu_pts), sum(int(p[0]) for p in gpu_pts)
     return {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port",
             "sample": f"CPU oracle (OpenMP over energies, OpenBLAS zgetrf/zgetri/dposv, radix-4 FFT; oracle/) on "
-                      f"{nthr} threads: real converged IV points of the same sweep at V = {volts[0]:g}..{volts[-1]:g} "
-                      f"(fresh start at the first) on {n_sample} energies over [-12,12] eV; value = the sample's "
-                      f"IV points/s x{n_sample}/{N_OMEGA}",
-            "sample_value": v_sample, "sample_s": t, "sample_converged": conv, "sample_energies": n_sample,
-            "scf_steps_per_point": [p["n_iter"] for p in pts],
-            "gpu_same_sample": {"form": "fp64", "device_s": gdev, "wall_s": gwall, "converged": gconv,
-                                "scf_steps_per_point": giters,
-                                "value": gconv / gdev if gdev > 0 else 0.0, "e2e": gconv / gwall if gwall > 0 else 0.0,
-                                "current_rel_diff_vs_cpu": float(np.max(np.abs(jg - jc)) / np.max(np.abs(jc)))}}
+                      f"{nthr} threads: {len(times)} SCF iterations (residual + Broyden update, full 16-column history) "
+                      f"of the same helix on {SAMPLE_N} of the 16384 energies, {np.mean(times):.3f} s each, x16 = "
+                      f"{t_it:.2f} s per full iteration; x {iters_per_point:.1f} SCF iterations per converged IV point "
+                      f"({ipp_note}); the initial and final sweeps of a point are not counted (in the CPU's favour)",
+            "seconds_per_iteration": t_it, "iterations_per_converged_point": iters_per_point,
+            "cfg0_real_sweep": {
+                "workload": "4x2 helix (16x16), U=0.5 eV, 4096 energies on [-10,10] eV, V 0..1 V step 0.1 with "
+                            "continuation, alpha_mix 0.1, tolf 1e-8, 16-column single-precision history",
+                "cpu": {"converged": cc, "wall_s": cpu_s, "value": cc / cpu_s if cpu_s > 0 else 0.0,
+                        "scf_steps_per_point": [p[1] for p in cpu_pts], "cores": nthr},
+                "gpu_fp64": {"converged": gc, "wall_s": gpu_s, "value": gc / gpu_s if gpu_s > 0 else 0.0,
+                             "scf_steps_per_point": [p[1] for p in gpu_pts]},
+                "gpu_over_cpu": (gc / gpu_s) / (cc / cpu_s) if cc and gpu_s > 0 else None,
+                "current_max_diff_rel": float(np.max(np.abs(jg[both] - jc[both])) / np.max(np.abs(jc[both])))
+                if both else None}}
 
 
 def observable_errors(ref_pts, pts):
@@ -297,44 +443,123 @@ def run_serving(qb, n_req, rate, max_inflight, precision):
             "converged": conv, "refused_too_large": len(refused), "failed": len(results) - len(ok),
             "p50_s": float(np.percentile(lat, 50)) if ok else None, "p99_s": float(np.percentile(lat, 99)) if ok else None,
             "mean_solve_s": float(np.mean([r["solve_s"] for r in ok])) if ok else None,
+            "mean_queue_s": float(np.mean([r["t_start"] - r["t_arrival"] for r in ok])) if ok else None,
+            "p50_service_s": float(np.percentile([r["t_done"] - r["t_start"] for r in ok], 50)) if ok else None,
+            "p99_service_s": float(np.percentile([r["t_done"] - r["t_start"] for r in ok], 99)) if ok else None,
+            "fp32_steps": int(sum(r["n_mixed"] for r in ok)), "scf_steps": int(sum(r["n_iter"] for r in ok)),
             "throughput_per_s": conv / span if span > 0 else 0.0, "span_s": span,
             "orbitals": [int(x[3]) for x in reqs]}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the oracle (a restatement of the reference's CPU path: OpenMP
-    over energies, LAPACK zgetrf/zgetri from OpenBLAS, its own FFT; oracle/) on all host
-    cores. Each step is a bounded sample of the workload: one real converged IV point of the
-    same sweep (same voltage, continuation, model, window and Broyden settings) on a grid of
-    --ref-sample energies. The line's value scales the measured rate to the 16384-energy
-    grid (scaled_cpu_rate); ms_per_step is the measured time of a sample step."""
+    """--impl reference: the oracle (a restatement of the reference's CPU path: OpenMP over
+    energies, LAPACK zgetrf/zgetri/dposv from OpenBLAS, its own FFT; oracle/, which loads
+    nothing of the product) on all host cores. Each step is a bounded sample of the workload:
+    one SCF iteration (residual + Broyden update with the full history) of the same helix,
+    window and settings on 1/16 of the energies, timed on its own. ms_per_step is that
+    measured time; the value converts it into converged IV points per second of the workload
+    with the x16 energy scale and the SCF iterations per converged point that the same sweep
+    window takes (SWEEP_ITERS_B200, the same algorithm in FP64 on B200)."""
     if rank != 0:
         return 0
     nthr = os.cpu_count()
     ions, turns = (int(v) for v in args.helix.split("x"))
-    block = voltage_block(0, 1)
-    seq = block[:args.warmup + args.steps]
+    seq = voltage_block(0, 1)[:args.warmup + args.steps]
+    window = seq[args.warmup:]
     t0 = time.perf_counter()
-    pts = cpu_sample_sweep(seq, args.ref_sample, threads=nthr, ions=ions, turns=turns)
-    timed = pts[args.warmup:]
-    v, v_sample, t, conv = scaled_cpu_rate(timed, args.ref_sample)
-    desc = (f"CPU oracle (OpenMP over energies, OpenBLAS zgetrf/zgetri/dposv, radix-4 FFT; oracle/) on {nthr} "
-            f"threads: {len(timed)} real converged IV points of the same sweep (voltages {timed[0]['V']:g}.."
-            f"{timed[-1]['V']:g}, continuation after {args.warmup} warm-up points) on {args.ref_sample} energies "
-            f"over [-12,12] eV: {conv} converged in {t:.1f} s = {v_sample:.4g} IV points/s; x{args.ref_sample}/"
-            f"{N_OMEGA} to the 16384-energy grid")
+    times = cpu_iteration_times(window[0], args.warmup + args.steps, args.ref_sample, threads=nthr, ions=ions,
+                                turns=turns)
+    timed = times[args.warmup:]
+    t_step = float(np.mean(timed)) if timed else 0.0
+    known = all(V in SWEEP_ITERS_B200 for V in window)
+    ipp = iters_per_converged_point(window, SWEEP_ITERS_B200, {V: SWEEP_ITERS_B200[V] < BROYDEN["maxscf"]
+                                                                for V in window}) if known else 0.0
+    scale = N_OMEGA / args.ref_sample
+    v = 1.0 / (t_step * scale * ipp) if known and timed and 0 < ipp < float("inf") else 0.0
+    desc = (f"CPU oracle (OpenMP over energies, OpenBLAS zgetrf/zgetri/dposv, radix-4 FFT; oracle/) on {nthr} threads: "
+            f"each step one SCF iteration (residual + Broyden update, full 16-column history) of the same helix on "
+            f"{args.ref_sample} of the 16384 energies ({t_step:.3f} s); value = 1 / (step x {scale:g} energies x "
+            f"{ipp:.1f} SCF iterations per converged IV point of voltages {window[0]:g}..{window[-1]:g}, measured on "
+            f"B200 with the same algorithm)")
     line = {"metric": "converged IV points/s", "value": v, "unit": "IV points/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / max(len(timed), 1),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": bench_config(args.n_omega, ions, turns, args.nhist, world),
             "cpu_baseline": {"value": v, "unit": "IV points/s", "cores": nthr, "kind": "port", "sample": desc,
-                             "sample_value": v_sample, "sample_energies": args.ref_sample,
-                             "scf_steps_per_point": [p["n_iter"] for p in timed],
-                             "converged": [bool(p["converged"]) for p in timed]},
+                             "seconds_per_full_iteration": t_step * scale, "iterations_per_converged_point": ipp},
             "e2e": {"value": v, "unit": "IV points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "run_s": time.perf_counter() - t0}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(finite(line), allow_nan=False), flush=True)
+    return 0
+
+
+def run_case(args, device):
+    """--case cfg2 / cfg4: the FP64 and mixed forms on a short sweep with continuation of the
+    multi-orbital molecule (make_cfg2_case: N = 248, nA = 128, 16384 energies instead of 32768,
+    8-column history) or of the 16 x 8 helix (N = nA = 256, lambda = 0.02 eV, U = 1.0 eV, 4096
+    energies on [-15, 15] eV instead of 65536, 4-column history): the full sizes need more
+    than one B200's HBM in FP64 (the SCF vectors and Broyden history alone exceed 180 GB)."""
+    import tempfile
+
+    import quichotte_b200 as qb
+    if args.case == "cfg2":
+        m = model_cfg2(qb, tempfile.mkdtemp(prefix="qs_cfg2_"), 16384)
+        nh, volts = 8, [0.1, 0.2, 0.3]
+        workload = ("synthetic 40-atom helicene-like molecule (28 C s,p + 12 H s; 248 spin-orbitals), dftb_hs form "
+                    "(S = I + P, ||P|| = 0.08; SOC xi = 0.00849 eV dual), U = 0.8 eV on 64 C orbitals (nA = 128), "
+                    "16384 energies over the spectrum +-1 eV; deviation: 16384 energies instead of 32768 and an "
+                    "8-column history (the full grid needs > 180 GB in FP64)")
+    else:
+        args4 = dict(N_ions=16, N_turns=8, hel_length=PITCH * 8 * 15 / 16, hel_radius=RADIUS, hand=1.0, E_CC=0.0,
+                     t_hop=1.0, lamb=0.02, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0)
+        ev = np.linalg.eigvalsh(qb.Model.helix(dw=1.0, up=1.0, delta=0.1, **args4).H)
+        n = 4096
+        delta = 30.0 / n
+        m = qb.Model.helix(dw=ev[0] + 15.0, up=15.0 - ev[-1] + 0.5 * delta, delta=delta, **args4)
+        nh, volts = 4, [-1.0, -0.95, -0.9]
+        workload = ("helix 16x8 (256x256 complex), lambda = 0.02 eV, U = 1.0 eV, 4096 energies on [-15,15] eV; "
+                    "deviation: 4096 energies instead of 65536 and a 4-column history (the full grid's SCF vectors "
+                    "alone are 4 x 103 GB), voltages solved one after another with continuation")
+    settings = dict(BROYDEN, nhist=nh)
+    out = {}
+    for prec, name in ((qb.QS_PREC_FP64, "fp64"), (qb.QS_PREC_MIXED, "mixed")):
+        s = qb.Solver(m, precision=prec, device=device, **settings)
+        s.profile(True)
+        pts, ok, dev = [], False, 0.0
+        t0 = time.perf_counter()
+        for k, V in enumerate(volts):
+            r = s.solve_scf(V, k == 0 or not ok)
+            ok = r["converged"]
+            dev += r["seconds"]
+            o = s.observables()
+            pts.append(dict(V=V, converged=ok, n_iter=r["n_iter"], n_mixed=r["n_mixed"], J=s.current(V),
+                            occ=np.imag(np.diag(o["G_less_obs"])).copy(), G=o["G_less_obs"], dosd=o["dosd"]))
+        wall = time.perf_counter() - t0
+        prof = s.profile(False)
+        out[name] = dict(points=pts, dev_s=dev, wall_s=wall, gib=s.device_gib(), nA=s.nA,
+                         kernel_ms={k: round(v[0], 3) for k, v in prof.items() if v[1]})
+        s.close()
+    f64, mix = out["fp64"], out["mixed"]
+    conv = lambda a: sum(int(p["converged"]) for p in a["points"])
+    line = {"metric": "converged IV points/s", "value": conv(mix) / mix["dev_s"] if mix["dev_s"] > 0 else 0.0,
+            "unit": "IV points/s", "n_gpus": 1, "steps": len(volts), "warmup": 0, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic", "case": args.case,
+            "config": {"workload": workload, "N": m.Norb, "nA": f64["nA"], "n_omega": m.n_omega, "nhist": nh,
+                       "voltages": volts},
+            "fp64": {"value": conv(f64) / f64["dev_s"] if f64["dev_s"] > 0 else 0.0, "device_s": f64["dev_s"],
+                     "converged": [p["converged"] for p in f64["points"]],
+                     "scf_steps_per_point": [p["n_iter"] for p in f64["points"]], "device_gib": f64["gib"],
+                     "kernel_ms": f64["kernel_ms"]},
+            "mixed": {"value": conv(mix) / mix["dev_s"] if mix["dev_s"] > 0 else 0.0, "device_s": mix["dev_s"],
+                      "converged": [p["converged"] for p in mix["points"]],
+                      "scf_steps_per_point": [p["n_iter"] for p in mix["points"]],
+                      "fp32_steps_per_point": [p["n_mixed"] for p in mix["points"]], "kernel_ms": mix["kernel_ms"]},
+            "mixed_over_fp64": (conv(mix) / mix["dev_s"]) / (conv(f64) / f64["dev_s"]) if conv(f64) and conv(mix)
+            else None,
+            "err_vs_fp64": observable_errors(f64["points"], mix["points"]),
+            "currents_A": [list(p["J"]) for p in f64["points"]]}
+    print(json.dumps(finite(line), allow_nan=False), flush=True)
     return 0
 
 
@@ -445,7 +670,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=SAMPLE_N, help="energies of the CPU sample grid")
-    ap.add_argument("--cpu-points", type=int, default=3, help="timed voltages in the GPU arm's CPU sample")
+    ap.add_argument("--cpu-iters", type=int, default=3, help="SCF iterations timed in the GPU arm's CPU sample")
     ap.add_argument("--n-omega", type=int, default=N_OMEGA, help="smaller grids for profiling only")
     ap.add_argument("--nhist", type=int, default=BROYDEN["nhist"], help="smaller histories for profiling only")
     ap.add_argument("--helix", default=f"{N_IONS}x{N_TURNS}", help="sites/turn x turns; other sizes for profiling only")
@@ -457,6 +682,12 @@ def main():
     ap.add_argument("--serve-inflight", type=int, default=4, help="solves on the device at once")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="both: the FP64 form, then the mixed form (headline value), with their ratio")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving stream (--serve requests at --serve-rate), FP64 then mixed, and print "
+                         "its line")
+    ap.add_argument("--case", default="cfg1", choices=["cfg1", "cfg2", "cfg4"],
+                    help="cfg1: the workload above (default); cfg2 / cfg4: the multi-orbital molecule and the "
+                         "256-state helix at the reduced sizes one B200 holds (their line names the deviation)")
     ap.add_argument("--setup-scan", action="store_true",
                     help="time the device set-up (eigenproblem, Loewdin) over sizes against LAPACK, print, exit")
     args = ap.parse_args()
@@ -470,6 +701,19 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.case != "cfg1":
+        return run_case(args, local)
+    if args.serve_only:
+        import quichotte_b200 as qb
+        line = {"metric": "served IV-point requests: p50/p99 latency and throughput", "case": "cfg3",
+                "workload": (f"first {args.serve} of the seeded 512-request stream: random helices, sites/turn 3-12, "
+                             "turns 1-8, U 0.2-1.5 eV, V -1..1 V, 4096-32768 energies on [-10,10] eV, Poisson "
+                             f"arrivals at {args.serve_rate}/s, {args.serve_inflight} solves in flight; one fresh-start "
+                             "IV point per request, Broyden nhist 8; requests above the HBM budget are refused")}
+        for name, prec in (("fp64", qb.QS_PREC_FP64), ("mixed", qb.QS_PREC_MIXED)):
+            line[name] = run_serving(qb, args.serve, args.serve_rate, args.serve_inflight, prec)
+        print(json.dumps(finite(line), allow_nan=False), flush=True)
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -620,9 +864,14 @@ def main():
         if world == 1:
             line["setup"] = setup_timing(qb, m)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_line(qb, seq[args.warmup:args.warmup + args.cpu_points], args.ref_sample,
-                                                     ions, turns, local)
-        print(json.dumps(line), flush=True)
+            ref_pts = (f64 or head)["points"]
+            its = sum(p["n_iter"] for p in ref_pts)
+            conv = sum(int(p["converged"]) for p in ref_pts)
+            ipp = its / conv if conv else 0.0
+            line["cpu_baseline"] = cpu_baseline_line(
+                qb, seq[args.warmup], args.cpu_iters, ions, turns, local, ipp,
+                f"this run's {'FP64' if f64 else prec_name} sweep: {its} iterations, {conv} converged points")
+        print(json.dumps(finite(line), allow_nan=False), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0

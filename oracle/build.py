@@ -1,6 +1,7 @@
 """Build recipe of the CPU oracle (TEST INFRASTRUCTURE; see oracle.cpp).
 
-    python oracle/build.py        -> oracle/_build/liboracle.so, oracle/_build/quichotte_oracle
+    python oracle/build.py        -> oracle/_build/liboracle.so, oracle/_build/quichotte_oracle,
+                                     oracle/_build/sancho_oracle
 
 The oracle links LAPACK/BLAS from the OpenBLAS inside the numpy wheel (ILP64 symbols
 scipy_*_64_), the only LAPACK in this image. It also links the host layer of the product
@@ -40,11 +41,13 @@ def build(verbose=False):
     run(["g++", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17",
          os.path.join(HERE, "oracle.cpp"), "-o", lib,
          "-L" + obdir, "-l:" + obname, "-Wl,-rpath," + obdir])
+    for name, main in (("quichotte_oracle", "oracle_main.cpp"), ("sancho_oracle", "sancho_oracle_main.cpp")):
+        exe = os.path.join(OUT, name)
+        run(["g++", "-O2", "-std=c++17", os.path.join(HERE, main), "-o", exe,
+             "-I" + os.path.join(ROOT, "include"),
+             "-L" + OUT, "-loracle", "-L" + HOSTLIB, "-lqs_host", "-fopenmp",
+             "-Wl,-rpath," + OUT, "-Wl,-rpath," + HOSTLIB, "-Wl,-rpath," + obdir])
     exe = os.path.join(OUT, "quichotte_oracle")
-    run(["g++", "-O2", "-std=c++17", os.path.join(HERE, "oracle_main.cpp"), "-o", exe,
-         "-I" + os.path.join(ROOT, "include"),
-         "-L" + OUT, "-loracle", "-L" + HOSTLIB, "-lqs_host", "-fopenmp",
-         "-Wl,-rpath," + OUT, "-Wl,-rpath," + HOSTLIB, "-Wl,-rpath," + obdir])
     if verbose:
         print("built", lib, exe)
     return lib, exe

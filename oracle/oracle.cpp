@@ -723,9 +723,8 @@ static void check_diag_sanity(const cplx *Grd, const cplx *GLd, int nb, int nw, 
         }
         double nocc = (-IM * HBAR * (delta / (2.0 * PI)) * sl).real();
         double wsum = -HBAR * (delta / PI) * si;
-        if (!std::isfinite(nocc) || !std::isfinite(wsum)) {
+        if (!std::isfinite(nocc) || !std::isfinite(wsum)) {  // runaway only: the return skips the last line
             runaway = true;
-            unphysical = true;
             i_worst = lab;
             n_worst = nocc;
             w_worst = wsum;
@@ -811,6 +810,10 @@ static void scf_residual1(qso_state &s, int64_t n, const double *x, double *F, b
     for (int64_t i = 0; i < n; i++) F[i] -= x[i];
 }
 
+// wall-clock time (s, steady clock) at the start of every Broyden iteration, recorded while
+// qso_solve_scf_timed runs (CPU-baseline timing only)
+static std::vector<double> *g_step_times = nullptr;
+
 // broyden_solve (common/broyden_mixing.f90:51-184), with its dot_ss / dot_sd (186-215)
 template <class Residual>
 static void broyden_solve(Residual residual, double *x, int64_t n, double alpha_mix, int nhist, int maxscf, double tolf,
@@ -834,6 +837,9 @@ static void broyden_solve(Residual residual, double *x, int64_t n, double alpha_
     n_resets = 0;
     for (int its = 1; its <= maxscf; its++) {
         n_iter = its;
+        if (g_step_times)
+            g_step_times->push_back(
+                std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
         bool abort = false;
         residual(n, x, F.data(), abort);
         if (abort) break;
@@ -1195,5 +1201,499 @@ int qso_fft(int n, double *data, int sign) {
     return 0;
 }
 int qso_good_fft_size(int nmin) { return good_fft_size(nmin); }
+
+// Timing helper of the CPU baseline (not a reference routine): qso_solve_scf with the wall
+// time of every SCF iteration (residual + Broyden update) in step_seconds[0 .. n-1]; returns
+// the number of iterations recorded (at most cap) or a negative status.
+int qso_solve_scf_timed(qso_state *s, double Volt, int fresh_start, qs_scf_result *res, double *step_seconds,
+                        int cap) {
+    std::vector<double> t;
+    g_step_times = &t;
+    int rc = qso_solve_scf(s, Volt, fresh_start, res);
+    g_step_times = nullptr;
+    if (rc) return rc < 0 ? rc : -rc;
+    t.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count());
+    int k = 0;
+    for (; k + 1 < (int)t.size() && k < cap; k++) step_seconds[k] = t[k + 1] - t[k];
+    // the last interval also holds the final sweep: drop it
+    return std::max(0, k - 1);
+}
+
+// Timing helper of the CPU baseline (not a reference routine): seconds of one broyden_solve
+// iteration without its residual, on a vector of n elements with a full history of nhist
+// columns (single or double precision). The residual is a cheap contraction whose own time
+// is measured and subtracted; the iterations after the history has filled are averaged. The
+// residual moves its fixed point every call, so every step stores a history pair.
+double qso_broyden_seconds_per_step(int64_t n, int nhist, int single) {
+    using clk = std::chrono::steady_clock;
+    const int steps = nhist + 4;
+    std::vector<double> x(n, 0.0);
+    std::vector<clk::time_point> t_call;
+    std::vector<double> t_res;
+    auto res = [&](int64_t nn, const double *xx, double *F, bool &ab) {
+        auto t0 = clk::now();
+        const double ph = 0.1 * (double)t_call.size();  // a moving target: F never vanishes
+        t_call.push_back(t0);
+#pragma omp parallel for
+        for (int64_t i = 0; i < nn; i++) F[i] = 0.5 * (std::sin(1e-3 * (double)(i % 1000) + ph) - xx[i]);
+        ab = false;
+        t_res.push_back(std::chrono::duration<double>(clk::now() - t0).count());
+    };
+    bool conv;
+    int it, resets;
+    double fmax;
+    std::vector<qs_scf_step> log;
+    broyden_solve(res, x.data(), n, 0.5, nhist, steps, 0.0, single != 0, conv, it, fmax, log, resets);
+    // interval between residual calls k and k+1 = residual k + the Broyden update of step k
+    double s = 0.0;
+    int cnt = 0;
+    for (int k = nhist + 1; k + 1 < (int)t_call.size(); k++) {
+        s += std::chrono::duration<double>(t_call[k + 1] - t_call[k]).count() - t_res[k];
+        cnt++;
+    }
+    return cnt ? s / cnt : 0.0;
+}
+
+}  // extern "C"
+
+// =====================================================================================
+// SANCHO (SANCHO/src): the spinless chain to third order in U. TEST INFRASTRUCTURE, as the
+// rest of this file: the checker of the B200 SANCHO solver (include/qsa200.h), exported as
+// qsao_*. Paths below are relative to the reference project's SANCHO/ directory; the common/
+// routines (pack_gf, invert_complex, broyden_solve) are the ones restated above.
+// =====================================================================================
+#include "../include/qsa200.h"
+
+struct qsao_state {
+    int Na = 0, n = 0, order = 0;
+    std::vector<cplx> H, GammaL, GammaR;
+    std::vector<double> U, omega;
+    double mu = 0, beta = 0, delta = 0, alpha_mix = 0.3, tolf = 1e-6;
+    int nhist = 8, maxscf = 200;
+    // G_in, G_out: (Na, Na, n), element (a, b, k) at a + b Na + k Na^2
+    std::vector<cplx> Gr, Ga, GL, GG, Or, Oa, OL, OG;
+    std::vector<cplx> Glt0;  // G^<_ii(t=0)
+    // self-energies (Na, Na, n); bubbles chi(m, a, b), m = -(n-1)..n-1, and phi(q, a, b), q = 2..2n
+    std::vector<cplx> S2R, S2L, S2G, S3R, S3L, S3G;
+    std::vector<cplx> chiG, chiL, chiR, chiA, phiG, phiL, phiR, phiA;
+    int64_t n_vec = 0;
+    int n_full = 0, n_strict_upper = 0;
+    double V_scf = 0;
+    int scf_iter = 0;
+    int64_t singular = 0;
+    std::string err;
+    size_t ix(int a, int b, int k) const { return (size_t)a + (size_t)b * Na + (size_t)k * Na * Na; }
+};
+
+// fermi (src/green_functions.f90:46-53): no cap on the exponent here
+static double sa_fermi(const qsao_state &s, double w, double V) {
+    double arg = (w - s.mu + V / HBAR) * s.beta;
+    return 1.0 / (std::exp(HBAR * arg) + 1.0);
+}
+
+// G^a = (G^r)^dagger per energy
+static void sa_adjoint(const qsao_state &s, const std::vector<cplx> &R, std::vector<cplx> &A) {
+    for (int k = 0; k < s.n; k++)
+        for (int b = 0; b < s.Na; b++)
+            for (int a = 0; a < s.Na; a++) A[s.ix(a, b, k)] = std::conj(R[s.ix(b, a, k)]);
+}
+
+// noninteracting_gr_ga + noninteracting_gl_gg (src/green_functions.f90:55-96)
+static void sa_noninteracting(qsao_state &s, double Volt) {
+    const int Na = s.Na;
+    for (int k = 0; k < s.n; k++) {
+        std::vector<cplx> w1((size_t)Na * Na);
+        for (size_t q = 0; q < w1.size(); q++) w1[q] = -s.H[q] + 0.5 * (IM / HBAR) * (s.GammaL[q] + s.GammaR[q]);
+        for (int i = 0; i < Na; i++) w1[i + (size_t)i * Na] += HBAR * s.omega[k];
+        if (invert_complex(Na, w1.data()) != 0 && !s.singular) s.singular = k + 1;
+        for (int b = 0; b < Na; b++)
+            for (int a = 0; a < Na; a++) {
+                s.Gr[s.ix(a, b, k)] = w1[a + (size_t)b * Na];
+                s.Ga[s.ix(a, b, k)] = std::conj(w1[b + (size_t)a * Na]);
+            }
+        const double fL = sa_fermi(s, s.omega[k], Volt), fR = sa_fermi(s, s.omega[k], 0.0);
+        std::vector<cplx> SL((size_t)Na * Na), T((size_t)Na * Na, 0.0);
+        for (size_t q = 0; q < SL.size(); q++) SL[q] = IM * (fL * s.GammaL[q] + fR * s.GammaR[q]) / HBAR;
+        for (int b = 0; b < Na; b++)
+            for (int c = 0; c < Na; c++)
+                for (int a = 0; a < Na; a++) T[a + (size_t)b * Na] += s.Gr[s.ix(a, c, k)] * SL[c + (size_t)b * Na];
+        for (int b = 0; b < Na; b++)
+            for (int a = 0; a < Na; a++) {
+                cplx acc = 0.0;
+                for (int c = 0; c < Na; c++) acc += T[a + (size_t)c * Na] * s.Ga[s.ix(c, b, k)];
+                s.GL[s.ix(a, b, k)] = acc;
+                s.GG[s.ix(a, b, k)] = acc + s.Gr[s.ix(a, b, k)] - s.Ga[s.ix(a, b, k)];
+            }
+    }
+}
+
+// complete_input_gf (src/green_functions.f90:164-173)
+static void sa_complete_input(qsao_state &s) {
+    sa_adjoint(s, s.Gr, s.Ga);
+    for (size_t q = 0; q < s.Gr.size(); q++) s.GG[q] = s.GL[q] + s.Gr[q] - s.Ga[q];
+}
+
+// equal_time_lesser (src/green_functions.f90:98-114)
+static void sa_equal_time_lesser(qsao_state &s) {
+    const double pp = s.delta / (2.0 * PI);
+    for (int i = 0; i < s.Na; i++) {
+        cplx acc = 0.0;
+        for (int k = 0; k < s.n; k++) acc += s.GL[s.ix(i, i, k)];
+        s.Glt0[i] = acc * pp;
+    }
+}
+
+// compute_bubbles (src/self_energies.f90:49-115): chi at nu = m delta (k2 = k1 - m on the
+// grid), phi at Omega = 2 w_init + q delta (k2 = q - k1 on the grid); 0-based k here
+static void sa_bubbles(qsao_state &s, int ord) {
+    const int Na = s.Na, Nw = s.n, Nm = 2 * Nw - 1;
+    const double pp = s.delta / (2.0 * PI);
+    auto cx = [&](int m, int a, int b) { return (size_t)(m + Nw - 1) + (size_t)Nm * (a + (size_t)b * Na); };
+    s.chiG.assign((size_t)Nm * Na * Na, 0.0);
+    s.chiL = s.chiR = s.chiA = s.chiG;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int b = 0; b < Na; b++)
+        for (int a = 0; a < Na; a++)
+            for (int m = -(Nw - 1); m <= Nw - 1; m++) {
+                cplx s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+                for (int k1 = std::max(0, m); k1 <= std::min(Nw - 1, Nw - 1 + m); k1++) {
+                    const int k2 = k1 - m;
+                    s1 += s.GG[s.ix(a, b, k1)] * s.GL[s.ix(b, a, k2)];
+                    s2 += s.GL[s.ix(a, b, k1)] * s.GG[s.ix(b, a, k2)];
+                    s3 += s.Gr[s.ix(a, b, k1)] * s.GL[s.ix(b, a, k2)] + s.GL[s.ix(a, b, k1)] * s.Ga[s.ix(b, a, k2)];
+                    s4 += s.Ga[s.ix(a, b, k1)] * s.GL[s.ix(b, a, k2)] + s.GL[s.ix(a, b, k1)] * s.Gr[s.ix(b, a, k2)];
+                }
+                s.chiG[cx(m, a, b)] = s1 * pp;
+                s.chiL[cx(m, a, b)] = s2 * pp;
+                s.chiR[cx(m, a, b)] = s3 * pp;
+                s.chiA[cx(m, a, b)] = s4 * pp;
+            }
+    if (ord < 3) return;
+    const int Nq = 2 * Nw - 1;  // q = 2..2 Nw (1-based energies): q0 = q - 2 = k1 + k2 (0-based), 0..2Nw-2
+    s.phiG.assign((size_t)Nq * Na * Na, 0.0);
+    s.phiL = s.phiR = s.phiA = s.phiG;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int b = 0; b < Na; b++)
+        for (int a = 0; a < Na; a++)
+            for (int q0 = 0; q0 < Nq; q0++) {
+                cplx s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+                for (int k1 = std::max(0, q0 - (Nw - 1)); k1 <= std::min(Nw - 1, q0); k1++) {
+                    const int k2 = q0 - k1;
+                    s1 += s.GG[s.ix(a, b, k1)] * s.GG[s.ix(a, b, k2)];
+                    s2 += s.GL[s.ix(a, b, k1)] * s.GL[s.ix(a, b, k2)];
+                    s3 += s.Gr[s.ix(a, b, k1)] * s.GG[s.ix(a, b, k2)] + s.GL[s.ix(a, b, k1)] * s.Gr[s.ix(a, b, k2)];
+                    s4 += s.Ga[s.ix(a, b, k1)] * s.GG[s.ix(a, b, k2)] + s.GL[s.ix(a, b, k1)] * s.Ga[s.ix(a, b, k2)];
+                }
+                const size_t o = (size_t)q0 + (size_t)Nq * (a + (size_t)b * Na);
+                s.phiG[o] = s1 * pp;
+                s.phiL[o] = s2 * pp;
+                s.phiR[o] = s3 * pp;
+                s.phiA[o] = s4 * pp;
+            }
+}
+
+// second_order_sigma (src/self_energies.f90:117-147)
+static void sa_sigma2(qsao_state &s) {
+    const int Na = s.Na, Nw = s.n, Nm = 2 * Nw - 1;
+    const double pp = s.delta / (2.0 * PI);
+    const cplx c2 = -(IM * HBAR) * (IM * HBAR);
+    auto cx = [&](int m, int a, int b) { return (size_t)(m + Nw - 1) + (size_t)Nm * (a + (size_t)b * Na); };
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int j = 0; j < Na; j++)
+        for (int i = 0; i < Na; i++)
+            for (int iw = 0; iw < Nw; iw++) {
+                cplx aR = 0.0, aL = 0.0, aG = 0.0;
+                for (int m = std::max(iw - (Nw - 1), -(Nw - 1)); m <= std::min(iw, Nw - 1); m++) {
+                    const int kk = iw - m;
+                    aL += s.GL[s.ix(i, j, kk)] * s.chiL[cx(m, i, j)];
+                    aG += s.GG[s.ix(i, j, kk)] * s.chiG[cx(m, i, j)];
+                    aR += s.Gr[s.ix(i, j, kk)] * s.chiG[cx(m, i, j)] + s.GL[s.ix(i, j, kk)] * s.chiR[cx(m, i, j)];
+                }
+                const cplx f = c2 * s.U[i] * s.U[j] * pp;
+                s.S2R[s.ix(i, j, iw)] = f * aR;
+                s.S2L[s.ix(i, j, iw)] = f * aL;
+                s.S2G[s.ix(i, j, iw)] = f * aG;
+            }
+}
+
+// third_order_sigma (src/self_energies.f90:149-207)
+static void sa_sigma3(qsao_state &s) {
+    const int Na = s.Na, Nw = s.n, Nm = 2 * Nw - 1, Nq = 2 * Nw - 1;
+    const double pp = s.delta / (2.0 * PI);
+    const cplx c3 = -(IM * HBAR) * (IM * HBAR) * (IM * HBAR);
+    auto cx = [&](int m, int a, int b) { return (size_t)(m + Nw - 1) + (size_t)Nm * (a + (size_t)b * Na); };
+    auto px = [&](int q0, int a, int b) { return (size_t)q0 + (size_t)Nq * (a + (size_t)b * Na); };
+    std::vector<cplx> SG((size_t)Nm * Na * Na, 0.0), SL(SG), SR(SG), PG((size_t)Nq * Na * Na, 0.0), PL(PG), PR(PG);
+    // 2. D and E: products in frequency summed over the internal site k with U_k
+#pragma omp parallel for collapse(2)
+    for (int j = 0; j < Na; j++)
+        for (int i = 0; i < Na; i++)
+            for (int k = 0; k < Na; k++) {
+                const double u = s.U[k];
+                for (int m = 0; m < Nm; m++) {
+                    const int mm = m - (Nw - 1);
+                    SG[cx(mm, i, j)] += u * (s.chiR[cx(mm, i, k)] * s.chiG[cx(mm, k, j)] + s.chiG[cx(mm, i, k)] * s.chiA[cx(mm, k, j)]);
+                    SL[cx(mm, i, j)] += u * (s.chiR[cx(mm, i, k)] * s.chiL[cx(mm, k, j)] + s.chiL[cx(mm, i, k)] * s.chiA[cx(mm, k, j)]);
+                    SR[cx(mm, i, j)] += u * s.chiR[cx(mm, i, k)] * s.chiR[cx(mm, k, j)];
+                }
+                for (int q0 = 0; q0 < Nq; q0++) {
+                    PG[px(q0, i, j)] += u * (s.phiR[px(q0, i, k)] * s.phiG[px(q0, k, j)] + s.phiG[px(q0, i, k)] * s.phiA[px(q0, k, j)]);
+                    PL[px(q0, i, j)] += u * (s.phiR[px(q0, i, k)] * s.phiL[px(q0, k, j)] + s.phiL[px(q0, i, k)] * s.phiA[px(q0, k, j)]);
+                    PR[px(q0, i, j)] += u * s.phiR[px(q0, i, k)] * s.phiR[px(q0, k, j)];
+                }
+            }
+    // 3. convolution with the remaining GF: particle-hole G_ij(w - nu), particle-particle
+    // G_ji(Omega - w) with q0 = iw + kk (0-based)
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int j = 0; j < Na; j++)
+        for (int i = 0; i < Na; i++)
+            for (int iw = 0; iw < Nw; iw++) {
+                cplx aR = 0.0, aL = 0.0, aG = 0.0;
+                for (int m = std::max(iw - (Nw - 1), -(Nw - 1)); m <= std::min(iw, Nw - 1); m++) {
+                    const int kk = iw - m;
+                    aL += s.GL[s.ix(i, j, kk)] * SL[cx(m, i, j)];
+                    aG += s.GG[s.ix(i, j, kk)] * SG[cx(m, i, j)];
+                    aR += s.Gr[s.ix(i, j, kk)] * SG[cx(m, i, j)] + s.GL[s.ix(i, j, kk)] * SR[cx(m, i, j)];
+                }
+                for (int kk = 0; kk < Nw; kk++) {
+                    const int q0 = iw + kk;
+                    aL += s.GG[s.ix(j, i, kk)] * PL[px(q0, i, j)];
+                    aG += s.GL[s.ix(j, i, kk)] * PG[px(q0, i, j)];
+                    aR += s.Ga[s.ix(j, i, kk)] * PG[px(q0, i, j)] + s.GG[s.ix(j, i, kk)] * PR[px(q0, i, j)];
+                }
+                const cplx f = c3 * s.U[i] * s.U[j] * pp;
+                s.S3R[s.ix(i, j, iw)] = f * aR;
+                s.S3L[s.ix(i, j, iw)] = f * aL;
+                s.S3G[s.ix(i, j, iw)] = f * aG;
+            }
+}
+
+// build_self_energies (src/self_energies.f90:40-47)
+static void sa_self_energies(qsao_state &s) {
+    if (s.order >= 2) {
+        sa_bubbles(s, s.order);
+        sa_sigma2(s);
+    }
+    if (s.order == 3) sa_sigma3(s);
+}
+
+// interacting_gf (src/scf.f90:147-195) at every energy
+static void sa_interacting_sweep(qsao_state &s, double Volt) {
+    const int Na = s.Na;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < s.n; k++) {
+        std::vector<cplx> SR((size_t)Na * Na, 0.0), SL((size_t)Na * Na, 0.0), w1((size_t)Na * Na);
+        if (s.order == 1) {
+            for (int i = 0; i < Na; i++) SR[i + (size_t)i * Na] -= IM * HBAR * s.U[i] * s.Glt0[i];
+        } else if (s.order >= 2) {
+            for (int b = 0; b < Na; b++)
+                for (int a = 0; a < Na; a++) {
+                    SR[a + (size_t)b * Na] = s.S2R[s.ix(a, b, k)];
+                    SL[a + (size_t)b * Na] = s.S2L[s.ix(a, b, k)];
+                }
+            for (int j = 0; j < Na; j++) SR[j + (size_t)j * Na] -= IM * HBAR * s.U[j] * s.Glt0[j];
+            if (s.order == 3)
+                for (int b = 0; b < Na; b++)
+                    for (int a = 0; a < Na; a++) {
+                        SR[a + (size_t)b * Na] += s.S3R[s.ix(a, b, k)];
+                        SL[a + (size_t)b * Na] += s.S3L[s.ix(a, b, k)];
+                    }
+        }
+        const double w = s.omega[k];
+        for (size_t q = 0; q < w1.size(); q++) w1[q] = -s.H[q] + 0.5 * (IM / HBAR) * (s.GammaL[q] + s.GammaR[q]) - SR[q];
+        for (int i = 0; i < Na; i++) w1[i + (size_t)i * Na] += HBAR * w;
+        if (invert_complex(Na, w1.data()) != 0) {
+#pragma omp critical
+            if (!s.singular) s.singular = k + 1;
+        }
+        const double fL = sa_fermi(s, w, Volt), fR = sa_fermi(s, w, 0.0);
+        for (size_t q = 0; q < SL.size(); q++) SL[q] = IM * (fL * s.GammaL[q] + fR * s.GammaR[q]) / HBAR + SL[q];
+        std::vector<cplx> T((size_t)Na * Na, 0.0);
+        for (int b = 0; b < Na; b++)
+            for (int c = 0; c < Na; c++)
+                for (int a = 0; a < Na; a++) T[a + (size_t)b * Na] += w1[a + (size_t)c * Na] * SL[c + (size_t)b * Na];
+        for (int b = 0; b < Na; b++)
+            for (int a = 0; a < Na; a++) {
+                cplx acc = 0.0;
+                for (int c = 0; c < Na; c++) acc += T[a + (size_t)c * Na] * std::conj(w1[b + (size_t)c * Na]);
+                const cplx gr = w1[a + (size_t)b * Na], ga = std::conj(w1[b + (size_t)a * Na]);
+                s.Or[s.ix(a, b, k)] = gr;
+                s.Oa[s.ix(a, b, k)] = ga;
+                s.OL[s.ix(a, b, k)] = acc;
+                s.OG[s.ix(a, b, k)] = acc + gr - ga;
+            }
+    }
+}
+
+// check_gf_sanity (common/scf_checks.f90) on the diagonals of a (Na, Na, n) pair
+static void sa_sanity(const qsao_state &s, const std::vector<cplx> &R, const std::vector<cplx> &L, bool &runaway,
+                      bool &unphysical, int &i_worst, double &n_worst, double &w_worst) {
+    std::vector<cplx> rd((size_t)s.Na * s.n), ld((size_t)s.Na * s.n);
+    for (int k = 0; k < s.n; k++)
+        for (int i = 0; i < s.Na; i++) {
+            rd[i + (size_t)k * s.Na] = R[s.ix(i, i, k)];
+            ld[i + (size_t)k * s.Na] = L[s.ix(i, i, k)];
+        }
+    check_diag_sanity(rd.data(), ld.data(), s.Na, s.n, s.delta, runaway, unphysical, i_worst, n_worst, w_worst,
+                      nullptr);
+}
+
+// scf_residual (src/scf.f90:102-136)
+static void sa_residual(qsao_state &s, int64_t n, const double *x, double *F, bool &abort) {
+    s.scf_iter++;
+    unpack_gf(s.Gr.data(), s.GL.data(), x, s.n_full, s.n_strict_upper, s.Na, s.n);
+    sa_complete_input(s);
+    sa_equal_time_lesser(s);
+    sa_self_energies(s);
+    sa_interacting_sweep(s, s.V_scf);
+    bool unphys;
+    int iw;
+    double nw, ww;
+    sa_sanity(s, s.Or, s.OL, abort, unphys, iw, nw, ww);
+    if (abort) {
+        std::fill(F, F + n, 0.0);
+        return;
+    }
+    pack_gf(s.Or.data(), s.OL.data(), F, s.n_full, s.n_strict_upper, s.Na, s.n);
+    for (int64_t i = 0; i < n; i++) F[i] -= x[i];
+}
+
+extern "C" {
+
+int qsao_create(const qsa_problem *p, qsao_state **out) {
+    scipy_openblas_set_num_threads64_(1);
+    auto *s = new qsao_state();
+    s->Na = p->N_sites;
+    s->n = p->n_omega;
+    s->order = p->order;
+    const size_t nn = (size_t)s->Na * s->Na;
+    s->H.assign((const cplx *)p->H, (const cplx *)p->H + nn);
+    s->GammaL.assign((const cplx *)p->GammaL, (const cplx *)p->GammaL + nn);
+    s->GammaR.assign((const cplx *)p->GammaR, (const cplx *)p->GammaR + nn);
+    s->U.assign(p->U_site, p->U_site + s->Na);
+    s->omega.assign(p->omega, p->omega + s->n);
+    s->mu = p->mu;
+    s->beta = p->beta;
+    s->delta = p->delta;
+    s->alpha_mix = p->alpha_mix;
+    s->tolf = p->tolf;
+    s->nhist = p->nhist;
+    s->maxscf = p->maxscf;
+    const size_t tot = nn * s->n;
+    for (auto *v : {&s->Gr, &s->Ga, &s->GL, &s->GG, &s->Or, &s->Oa, &s->OL, &s->OG, &s->S2R, &s->S2L, &s->S2G, &s->S3R,
+                    &s->S3L, &s->S3G})
+        v->assign(tot, 0.0);
+    s->Glt0.assign(s->Na, 0.0);
+    // src/sancho.f90:106-109
+    s->n_full = (int)nn;
+    s->n_strict_upper = (s->n_full - s->Na) / 2;
+    s->n_vec = (int64_t)(2 * s->n_full + s->n_strict_upper + s->n_strict_upper + s->Na) * s->n;
+    *out = s;
+    return 0;
+}
+void qsao_destroy(qsao_state *s) { delete s; }
+const char *qsao_last_error(const qsao_state *s) { return s ? s->err.c_str() : "no handle"; }
+int64_t qsao_vector_length(const qsao_state *s) { return s->n_vec; }
+
+static int sa_check_singular(qsao_state *s) {
+    if (s->singular) {
+        s->err = "ERROR: ZGETRF failed (singular matrix?) at energy " + std::to_string(s->singular);
+        int e = (int)s->singular;
+        s->singular = 0;
+        return e;
+    }
+    return 0;
+}
+
+// solve_scf (src/scf.f90:53-95)
+int qsao_solve_scf(qsao_state *s, double Volt, int fresh_start, qs_scf_result *res) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (fresh_start) sa_noninteracting(*s, Volt);
+    if (int e = sa_check_singular(s)) return e;
+    std::vector<double> x(s->n_vec);
+    pack_gf(s->Gr.data(), s->GL.data(), x.data(), s->n_full, s->n_strict_upper, s->Na, s->n);
+    s->V_scf = Volt;
+    s->scf_iter = 0;
+    bool converged, aborted = false;
+    int n_iter = 0, n_resets = 0;
+    double fmax = 0.0;
+    std::vector<qs_scf_step> log;
+    broyden_solve([&](int64_t n, const double *xx, double *F, bool &ab) { sa_residual(*s, n, xx, F, ab); aborted = aborted || ab; },
+                  x.data(), s->n_vec, s->alpha_mix, s->nhist, s->maxscf, s->tolf, false, converged, n_iter, fmax, log,
+                  n_resets);
+    if (int e = sa_check_singular(s)) return e;
+    bool runaway, unphysical;
+    int i_worst;
+    double n_worst, w_worst;
+    sa_sanity(*s, s->Or, s->OL, runaway, unphysical, i_worst, n_worst, w_worst);
+    if (converged && unphysical) converged = false;
+    res->converged = converged && !aborted;
+    res->n_iter = n_iter;
+    res->fmax = fmax;
+    res->aborted = aborted;
+    res->runaway = runaway;
+    res->unphysical = unphysical;
+    res->i_worst = i_worst;
+    res->n_worst = n_worst;
+    res->w_worst = w_worst;
+    res->n_resets = n_resets;
+    res->n_log = 0;
+    for (auto &e : log)
+        if (res->log && res->n_log < res->log_cap) res->log[res->n_log++] = e;
+    res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    res->n_mixed = 0;
+    return 0;
+}
+
+// Current (src/observables.f90:18-52): 2 (delta/hbar) sum_w Re Tr{i GammaL [(fL - 1) G^< - fL G^>]}/2pi
+int qsao_current(qsao_state *s, double Volt, double *J) {
+    double JL = 0.0;
+    for (int k = 0; k < s->n; k++) {
+        const double fL = sa_fermi(*s, s->omega[k], Volt);
+        cplx tr = 0.0;
+        for (int a = 0; a < s->Na; a++)
+            for (int c = 0; c < s->Na; c++)
+                tr += IM * s->GammaL[a + (size_t)c * s->Na] *
+                      ((fL - 1.0) * s->GL[s->ix(c, a, k)] - fL * s->GG[s->ix(c, a, k)]);
+        JL += tr.real() / (2.0 * PI);
+    }
+    *J = 2.0 * JL * (s->delta / HBAR);
+    return 0;
+}
+
+int qsao_get_observables(qsao_state *s, double *G_less_t0, double *spectral) {
+    if (G_less_t0) std::memcpy(G_less_t0, s->Glt0.data(), sizeof(cplx) * s->Na);
+    if (spectral)
+        for (int k = 0; k < s->n; k++)
+            for (int i = 0; i < s->Na; i++) spectral[i + (size_t)k * s->Na] = -2.0 * s->Gr[s->ix(i, i, k)].imag();
+    return 0;
+}
+
+int qsao_initial_vector(qsao_state *s, double Volt, double *x) {
+    sa_noninteracting(*s, Volt);
+    pack_gf(s->Gr.data(), s->GL.data(), x, s->n_full, s->n_strict_upper, s->Na, s->n);
+    return sa_check_singular(s);
+}
+
+int qsao_residual(qsao_state *s, double Volt, const double *x, double *F, int *abort_flag) {
+    s->V_scf = Volt;
+    bool ab = false;
+    sa_residual(*s, s->n_vec, x, F, ab);
+    *abort_flag = ab;
+    return sa_check_singular(s);
+}
+
+int qsao_self_energies(qsao_state *s, const double *x, double *Sig2R, double *Sig2L, double *Sig3R, double *Sig3L) {
+    unpack_gf(s->Gr.data(), s->GL.data(), x, s->n_full, s->n_strict_upper, s->Na, s->n);
+    sa_complete_input(*s);
+    sa_equal_time_lesser(*s);
+    sa_self_energies(*s);
+    const size_t bytes = sizeof(cplx) * s->S2R.size();
+    if (Sig2R) std::memcpy(Sig2R, s->S2R.data(), bytes);
+    if (Sig2L) std::memcpy(Sig2L, s->S2L.data(), bytes);
+    if (Sig3R) std::memcpy(Sig3R, s->S3R.data(), bytes);
+    if (Sig3L) std::memcpy(Sig3L, s->S3L.data(), bytes);
+    return 0;
+}
 
 }  // extern "C"

@@ -133,6 +133,10 @@ def lib():
         L.qso_initial_vector.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
         L.qso_vector_length.argtypes = [ctypes.c_void_p]
         L.qso_vector_length.restype = ctypes.c_int64
+        L.qso_solve_scf_timed.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_Result),
+                                          ctypes.c_void_p, ctypes.c_int]
+        L.qso_broyden_seconds_per_step.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+        L.qso_broyden_seconds_per_step.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -170,6 +174,23 @@ class Solver:
         return {"converged": bool(r.converged), "n_iter": r.n_iter, "fmax": r.fmax, "aborted": r.aborted,
                 "unphysical": r.unphysical, "n_resets": r.n_resets, "wall": wall,
                 "log": [(log[i].step, log[i].fmax, log[i].rms, log[i].nh) for i in range(r.n_log)]}
+
+    def solve_timed(self, V, fresh_start=True):
+        """solve_scf with the wall time of every SCF iteration (residual + Broyden update):
+        returns (result as solve_scf, seconds per iteration; the final sweep excluded)."""
+        L = lib()
+        cap = self.maxscf + 2
+        log = (_Step * cap)()
+        r = _Result()
+        r.log, r.log_cap = log, cap
+        dt = np.zeros(cap)
+        k = L.qso_solve_scf_timed(self._h, V, int(fresh_start), ctypes.byref(r), dt.ctypes.data_as(ctypes.c_void_p),
+                                  cap)
+        if k < 0:
+            raise RuntimeError(f"qso_solve_scf_timed failed ({k})")
+        res = {"converged": bool(r.converged), "n_iter": r.n_iter, "aborted": r.aborted,
+               "log": [(log[i].step, log[i].fmax, log[i].rms, log[i].nh) for i in range(r.n_log)]}
+        return res, dt[:k].copy()
 
     def current(self, V):
         ju, jd = ctypes.c_double(), ctypes.c_double()

@@ -6,6 +6,7 @@ produces, under quichotte-and-sancho_b200/_build/:
     libqs_host.so    host layer: input.dat reader, model builders, output files, program flow
     libqsb200.so     the CUDA library (include/qsb200.h), compiled for sm_100a
     quichotte_b200   the QUICHOTTE program over libqsb200.so (drop-in for bin/quichotte.x)
+    sancho_b200      the SANCHO program over libqsb200.so (drop-in for SANCHO's bin/sancho.x)
 """
 import glob
 import os
@@ -40,9 +41,11 @@ def newer(target, sources):
 
 def build_host(verbose=False):
     os.makedirs(OUT, exist_ok=True)
-    srcs = [os.path.join(HERE, "host", f) for f in ("qs_host.cpp", "qs_main.cpp")]
+    srcs = [os.path.join(HERE, "host", f) for f in ("qs_host.cpp", "qs_main.cpp", "sancho_host.cpp")]
     lib = os.path.join(OUT, "libqs_host.so")
-    if not newer(lib, srcs + [os.path.join(INC, "qs_host.h"), os.path.join(INC, "qsb200.h")]):
+    hdrs = [os.path.join(HERE, "host", "host_common.hpp")] + [os.path.join(INC, h) for h in
+                                                               ("qs_host.h", "qsb200.h", "qsa200.h", "qsa_host.h")]
+    if not newer(lib, srcs + hdrs):
         run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I" + INC] + srcs + ["-o", lib], verbose)
     return lib
 
@@ -50,7 +53,8 @@ def build_host(verbose=False):
 def build_cuda(verbose=False, ptxas_verbose=False):
     os.makedirs(OUT, exist_ok=True)
     cu = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
-    hdr = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(INC, "qsb200.h")]
+    hdr = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(INC, "qsb200.h"),
+                                                                      os.path.join(INC, "qsa200.h")]
     lib = os.path.join(OUT, "libqsb200.so")
     if newer(lib, cu + hdr):
         return lib
@@ -72,13 +76,14 @@ def build_cuda(verbose=False, ptxas_verbose=False):
 
 
 def build_program(verbose=False):
-    exe = os.path.join(OUT, "quichotte_b200")
-    src = os.path.join(HERE, "host", "qs_gpu_main.cpp")
-    deps = [src, os.path.join(OUT, "libqs_host.so"), os.path.join(OUT, "libqsb200.so")]
-    if not newer(exe, deps):
-        run(["g++", "-O2", "-std=c++17", "-I" + INC, src, "-o", exe, "-L" + OUT, "-lqsb200", "-lqs_host",
-             "-Wl,-rpath," + OUT], verbose)
-    return exe
+    for name, main in (("quichotte_b200", "qs_gpu_main.cpp"), ("sancho_b200", "sancho_gpu_main.cpp")):
+        exe = os.path.join(OUT, name)
+        src = os.path.join(HERE, "host", main)
+        deps = [src, os.path.join(OUT, "libqs_host.so"), os.path.join(OUT, "libqsb200.so")]
+        if not newer(exe, deps):
+            run(["g++", "-O2", "-std=c++17", "-I" + INC, src, "-o", exe, "-L" + OUT, "-lqsb200", "-lqs_host",
+                 "-Wl,-rpath," + OUT], verbose)
+    return os.path.join(OUT, "quichotte_b200")
 
 
 def build(verbose=False):

@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(256) vec_norms(const double *__restrict__ F, c
 // (common/broyden_mixing.f90:103-138,150-156). Single-precision history stores
 // real(dF/||dF||) and real(alpha dF/||dF|| + dx/||dF||); every dot accumulates in FP64.
 // Each thread handles groups of 4 consecutive elements (vector loads); n % 4 elements at
-// the end are handled one by one.
+// the end are handled one by one. History columns are ld = broyden_ld(n) elements apart (n
+// rounded up to a multiple of 4), so every column starts on a 16-byte boundary.
 template <typename HT> struct V4;
 template <> struct V4<float> { using t = float4; };
 template <> struct V4<double> { using t = double4; };
@@ -139,9 +140,9 @@ __device__ __forceinline__ void hist_elem(double f, double fo, double xx, double
 template <typename HT, int NH>
 __global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
                                                       const double *__restrict__ x, const double *__restrict__ xold,
-                                                      int64_t n, double fnorm, double alpha, HT *__restrict__ dF,
-                                                      HT *__restrict__ U, int slot, int nh, int store,
-                                                      double *__restrict__ part) {
+                                                      int64_t n, int64_t ld, double fnorm, double alpha,
+                                                      HT *__restrict__ dF, HT *__restrict__ U, int slot, int nh,
+                                                      int store, double *__restrict__ part) {
     __shared__ double sh[2 * NH * 8];
     double g[NH], c[NH];
 #pragma unroll
@@ -175,11 +176,11 @@ __global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__
             for (int e = 0; e < 4; e++)
                 if (e < cnt) hist_elem<HT>(f[e], fo[e], xx[e], xo[e], fnorm, rf, alpha, dnew[e], unew[e]);
             if (vec) {
-                hst4<HT>(dF + (int64_t)slot * n + i0, dnew);
-                hst4<HT>(U + (int64_t)slot * n + i0, unew);
+                hst4<HT>(dF + (int64_t)slot * ld + i0, dnew);
+                hst4<HT>(U + (int64_t)slot * ld + i0, unew);
             } else {
-                dF[(int64_t)slot * n + i0] = dnew[0];
-                U[(int64_t)slot * n + i0] = unew[0];
+                dF[(int64_t)slot * ld + i0] = dnew[0];
+                U[(int64_t)slot * ld + i0] = unew[0];
             }
         }
 #pragma unroll
@@ -192,9 +193,9 @@ __global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__
 #pragma unroll
                     for (int e = 0; e < 4; e++) dk[e] = dn[e];
                 } else if (vec) {
-                    hld4<HT>(dF + (int64_t)k * n + i0, dk);
+                    hld4<HT>(dF + (int64_t)k * ld + i0, dk);
                 } else {
-                    dk[0] = (double)dF[(int64_t)k * n + i0];
+                    dk[0] = (double)dF[(int64_t)k * ld + i0];
                 }
 #pragma unroll
                 for (int e = 0; e < 4; e++)
@@ -230,14 +231,15 @@ __global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__
 template <typename HT>
 static void launch_hist(int nb, cudaStream_t st, const double *F, const double *Fold, const double *x, const double *xold,
                         int64_t n, double fnorm, double alpha, HT *dF, HT *U, int slot, int nh, int store, double *part) {
+    const int64_t ld = broyden_ld(n);
     if (nh <= 4)
-        hist_update<HT, 4><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update<HT, 4><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
     else if (nh <= 8)
-        hist_update<HT, 8><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update<HT, 8><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
     else if (nh <= 16)
-        hist_update<HT, 16><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update<HT, 16><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
     else
-        hist_update<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
 }
 
 // x_new = x + alpha F - sum_k gamma_k U_k   (common/broyden_mixing.f90:165-178), the
@@ -245,7 +247,7 @@ static void launch_hist(int nb, cudaStream_t st, const double *F, const double *
 template <typename HT>
 __global__ void __launch_bounds__(256) x_update(const double *__restrict__ x, const double *__restrict__ F,
                                                 const HT *__restrict__ U, const double *__restrict__ gam, int nh,
-                                                double alpha, int64_t n, double *__restrict__ xnew) {
+                                                double alpha, int64_t n, int64_t ld, double *__restrict__ xnew) {
     __shared__ double gs[MAXH];
     if (threadIdx.x < nh) gs[threadIdx.x] = gam[threadIdx.x];
     __syncthreads();
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(256) x_update(const double *__restrict__ x, co
         double r[4] = {xv.x + alpha * fv.x, xv.y + alpha * fv.y, xv.z + alpha * fv.z, xv.w + alpha * fv.w};
         for (int k = 0; k < nh; k++) {
             double u[4];
-            hld4<HT>(U + (int64_t)k * n + i0, u);
+            hld4<HT>(U + (int64_t)k * ld + i0, u);
 #pragma unroll
             for (int e = 0; e < 4; e++) r[e] -= u[e] * gs[k];
         }
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(256) x_update(const double *__restrict__ x, co
     }
     for (int64_t i = 4 * n4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         double xi = x[i] + alpha * F[i];
-        for (int k = 0; k < nh; k++) xi -= (double)U[(int64_t)k * n + i] * gs[k];
+        for (int k = 0; k < nh; k++) xi -= (double)U[(int64_t)k * ld + i] * gs[k];
         xnew[i] = xi;
     }
 }
@@ -404,9 +406,9 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
         // x_new into the xold buffer, then rotate: xold <- x, x <- x_new, Fold <- F
         int pk = prof_begin(h, K_BROYDEN);
         if (sp)
-            x_update<float><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const float *)d_hU, gam, nh, alpha_mix, n, d_xold);
+            x_update<float><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const float *)d_hU, gam, nh, alpha_mix, n, broyden_ld(n), d_xold);
         else
-            x_update<double><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const double *)d_hU, gam, nh, alpha_mix, n, d_xold);
+            x_update<double><<<nb, RED_THREADS, 0, st>>>(d_x, d_F, (const double *)d_hU, gam, nh, alpha_mix, n, broyden_ld(n), d_xold);
         prof_end(h, pk);
         QS_CUDA(h, cudaGetLastError());
         std::swap(d_x, d_xold);

@@ -286,6 +286,18 @@ int invert_batched_ws(cudaStream_t st, int N, int batch, zc *d_A, int *d_min_inf
 int convert_ref_to_dl(cudaStream_t st, int nA, int64_t Nw, const double *ref, double *dl);
 int convert_dl_to_ref(cudaStream_t st, int nA, int64_t Nw, const double *dl, double *ref);
 
+// check_diag_sanity (common/scf_checks.f90:59-91) from the per-state sums over energies:
+// sumL[i] = sum_w G^<_ii(w), sumRim[i] = sum_w Im G^r_ii(w); state_index maps i to the
+// reported (0-based) state label, or nullptr for i itself
+struct SanityOut {
+    bool runaway = false, unphysical = false;
+    int i_worst = 1;
+    double n_worst = 0.5, w_worst = 1.0;
+};
+SanityOut check_diag_sanity(int nb, const std::vector<zc> &sumL, const std::vector<double> &sumRim, double delta,
+                            const int *state_index);
+void release_all(qs_handle *h);
+
 // Broyden (common/broyden_mixing.f90) on device vectors; the residual is a host callback
 // that fills F (device) from x (device) and may set abort.
 struct BroydenResidual {
@@ -302,6 +314,9 @@ struct BroydenOut {
     bool aborted = false;
     std::vector<qs_scf_step> log;
 };
+// column stride (elements) of the Broyden history: n rounded up to a multiple of 4, so that
+// every column starts on a 16-byte boundary for the kernels' 4-wide vector accesses
+inline int64_t broyden_ld(int64_t n) { return (n + 3) & ~(int64_t)3; }
 int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *&d_F, double *&d_Fold,
                       double *&d_xold, void *d_hdF, void *d_hU, int64_t n, double alpha_mix, int nhist, int maxscf,
                       double tolf, bool sp, BroydenOut &out);

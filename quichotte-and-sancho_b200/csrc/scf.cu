@@ -138,13 +138,7 @@ using namespace qs;
 // ------------------------------------------------------------------------------------
 // host helpers
 // ------------------------------------------------------------------------------------
-namespace {
-
-struct SanityOut {
-    bool runaway = false, unphysical = false;
-    int i_worst = 1;
-    double n_worst = 0.5, w_worst = 1.0;
-};
+namespace qs {
 
 // check_diag_sanity (common/scf_checks.f90:59-91) from the per-state sums over energies:
 // sumL[i] = sum_w G^<_ii(w), sumRim[i] = sum_w Im G^r_ii(w).
@@ -155,8 +149,8 @@ SanityOut check_diag_sanity(int nb, const std::vector<zc> &sumL, const std::vect
         int lab = state_index ? state_index[i] + 1 : i + 1;
         double nocc = 1.0 * (delta / (2.0 * PI)) * sumL[i].y;  // Re(-i hbar pp sum)
         double wsum = -1.0 * (delta / PI) * sumRim[i];
-        if (!std::isfinite(nocc) || !std::isfinite(wsum)) {
-            s.runaway = s.unphysical = true;
+        if (!std::isfinite(nocc) || !std::isfinite(wsum)) {  // runaway only, as the reference returns here
+            s.runaway = true;
             s.i_worst = lab;
             s.n_worst = nocc;
             s.w_worst = wsum;
@@ -173,6 +167,10 @@ SanityOut check_diag_sanity(int nb, const std::vector<zc> &sumL, const std::vect
     if (s.runaway) s.unphysical = true;
     return s;
 }
+
+}  // namespace qs
+
+namespace {
 
 int read_info(qs_handle *h, int &info) {
     int hv[2];
@@ -284,16 +282,18 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
     return 0;
 }
 
-// The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: the leading steps form the
-// second-order self-energies in FP32 (FFTs, 2x2 algebra and spectra) and the Keldysh
-// products on the tensor cores (3xTF32, keldysh_tf32.cu); once max|F| falls below
-// mixed_switch = max(1e-5, 100 tolf), or has not improved for five steps, the solve
-// continues in FP64 (an FP32 step whose max|F| is already below tolf is redone in FP64
-// first, so that it cannot end the solve). The FP32 self-energies leave a noise floor of
-// about 1e-5 in F on the 120x120 helix, so FP32 steps stop well above it. Convergence
-// (max|F| < tolf) is always decided on an FP64 residual, and the converged state meets the
-// FP64 solve's criterion. The Broyden pair of the first FP64 step (its dF is an FP64
-// residual minus an FP32 one) is not stored (precision_changed).
+// The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: while max|F| is far above the
+// FP32 noise floor, the steps form the second-order self-energies in FP32 (FFTs, 2x2
+// algebra and spectra) and the Keldysh products on the tensor cores (3xTF32,
+// keldysh_tf32.cu). The FP32 self-energies leave a noise floor of about 1e-5 in F on the
+// 120x120 helix. The solve continues in FP64 once max|F| falls below mixed_switch =
+// max(1e-5, 100 tolf), or once it has not improved for five steps while below
+// 100 mixed_switch (near the floor, where FP32 noise could stall it; far above it a stalling
+// solve gains nothing from FP64). An FP32 step whose max|F| is already below tolf is redone in
+// FP64 first, so that it cannot end the solve: convergence (max|F| < tolf) is always decided
+// on an FP64 residual, and the converged state meets the FP64 solve's criterion. The Broyden
+// pair of the first FP64 step (its dF is an FP64 residual minus an FP32 one) is not stored
+// (precision_changed).
 struct Residual2 : BroydenResidual {
     qs_handle *h;
     double V;
@@ -332,7 +332,7 @@ struct Residual2 : BroydenResidual {
             since_best++;
         }
         n_mixed++;
-        if (fmax < h->mixed_switch || since_best >= 5 || iter >= h->maxscf / 2) {
+        if (fmax < h->mixed_switch || (since_best >= 5 && fmax < 100.0 * h->mixed_switch)) {
             fp32 = false;  // the next steps are FP64
             if (fmax < h->tolf) {  // never let an FP32 residual declare convergence: redo it
                 n_mixed--;
@@ -565,7 +565,7 @@ static size_t handle_need(const qs_handle *h) {
     if (h->order == 2) {
         size_t nY = (size_t)nA * nA + (size_t)nA * (nA + 1) / 2;
         need += (size_t)h->n_vec * 8 * 4;                                     // x, F, Fold, xold
-        need += (size_t)h->n_vec * hist_el * 2 * h->nhist;                    // history
+        need += (size_t)broyden_ld(h->n_vec) * hist_el * 2 * h->nhist;                    // history
         need += (size_t)n * nA * nA * zc_ * 2;                                // SigR, SigL
         need += (nY + (size_t)2 * nA * nA) * Nf * zc_;                        // Y, V
     } else {
@@ -573,7 +573,7 @@ static size_t handle_need(const qs_handle *h) {
         need += G_chunk * nn * zc_;                                           // full-G chunk
         need += (size_t)148 * 4 * N * std::max(h->nS, 1) * zc_;               // sweep scratch
         const int64_t nv = std::max<int64_t>(h->n_vec, 1);
-        if (h->order == 1) need += (size_t)nv * 8 * 4 + (size_t)nv * hist_el * 2 * h->nhist;
+        if (h->order == 1) need += (size_t)nv * 8 * 4 + (size_t)broyden_ld(nv) * hist_el * 2 * h->nhist;
     }
     need += broyden_red_len() * 8 + (size_t)3 * h->nS * h->nS * zc_;        // reductions, Gamma blocks
     if (h->order == 2) {
@@ -671,8 +671,8 @@ int qs_create(const qs_problem *p, qs_handle **out) {
         if ((rc = dalloc(h, (void **)&h->d_x, h->n_vec * 8)) || (rc = dalloc(h, (void **)&h->d_F, h->n_vec * 8)) ||
             (rc = dalloc(h, (void **)&h->d_Fold, h->n_vec * 8)) || (rc = dalloc(h, (void **)&h->d_xold, h->n_vec * 8)))
             return rc;
-        if (h->nhist > 0 && ((rc = dalloc(h, &h->d_hdF, h->n_vec * hist_el * h->nhist)) ||
-                             (rc = dalloc(h, &h->d_hU, h->n_vec * hist_el * h->nhist))))
+        if (h->nhist > 0 && ((rc = dalloc(h, &h->d_hdF, broyden_ld(h->n_vec) * hist_el * h->nhist)) ||
+                             (rc = dalloc(h, &h->d_hU, broyden_ld(h->n_vec) * hist_el * h->nhist))))
             return rc;
         if ((rc = sigma2_setup(h))) return rc;
         h->d_G = h->d_Y;
@@ -686,8 +686,8 @@ int qs_create(const qs_problem *p, qs_handle **out) {
             if ((rc = dalloc(h, (void **)&h->d_x, nv * 8)) || (rc = dalloc(h, (void **)&h->d_F, nv * 8)) ||
                 (rc = dalloc(h, (void **)&h->d_Fold, nv * 8)) || (rc = dalloc(h, (void **)&h->d_xold, nv * 8)))
                 return rc;
-            if (h->nhist > 0 && ((rc = dalloc(h, &h->d_hdF, nv * hist_el * h->nhist)) ||
-                                 (rc = dalloc(h, &h->d_hU, nv * hist_el * h->nhist))))
+            if (h->nhist > 0 && ((rc = dalloc(h, &h->d_hdF, broyden_ld(nv) * hist_el * h->nhist)) ||
+                                 (rc = dalloc(h, &h->d_hU, broyden_ld(nv) * hist_el * h->nhist))))
                 return rc;
         }
         h->G_chunk = std::max<size_t>(1, std::min<size_t>((size_t)n, (2ull << 30) / (nn * zc_)));
@@ -1080,7 +1080,7 @@ int qs_broyden_solve_host(qs_residual_fn residual, void *ctx, double *x, int64_t
     if ((rc = dalloc(&h, (void **)&h.d_x, n * 8)) || (rc = dalloc(&h, (void **)&h.d_F, n * 8)) ||
         (rc = dalloc(&h, (void **)&h.d_Fold, n * 8)) || (rc = dalloc(&h, (void **)&h.d_xold, n * 8)) ||
         (rc = dalloc(&h, (void **)&h.d_red, h.red_len * 8)) ||
-        (nhist > 0 && ((rc = dalloc(&h, &h.d_hdF, n * hist_el * nhist)) || (rc = dalloc(&h, &h.d_hU, n * hist_el * nhist))))) {
+        (nhist > 0 && ((rc = dalloc(&h, &h.d_hdF, broyden_ld(n) * hist_el * nhist)) || (rc = dalloc(&h, &h.d_hU, broyden_ld(n) * hist_el * nhist))))) {
     } else {
         cudaMemcpyAsync(h.d_x, x, sizeof(double) * n, cudaMemcpyHostToDevice, h.stream);
         HostResidual r;

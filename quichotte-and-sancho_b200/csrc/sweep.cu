@@ -205,8 +205,8 @@ __host__ __device__ __forceinline__ int swz_units(int N) { return N * swz_ld(N);
 // thread for the panel's register-resident rows
 constexpr int BGJ_THREADS = 480;
 
-// named barrier of the 4 panel warps (ids 1.. are free; 0 is __syncthreads)
-__device__ __forceinline__ void panel_bar() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+// named barrier of the panel warps (ids 1.. are free; 0 is __syncthreads)
+__device__ __forceinline__ void panel_bar(int nthreads) { asm volatile("bar.sync 1, %0;\n" ::"r"(nthreads) : "memory"); }
 
 // argmax over a warp with the result in every lane (first maximum wins)
 __device__ __forceinline__ void warp_argmax_all(double &v, int &i) {
@@ -221,9 +221,20 @@ __device__ __forceinline__ void warp_argmax_all(double &v, int &i) {
     }
 }
 
-// Blocked Gauss-Jordan inversion for 16 <= N <= 128 with the matrix in (swizzled) shared
-// memory. Per panel K = [k0, k0 + 16):
-//   panel   warps 0-3, thread i holding row i of the panel columns in registers: per column
+// Storage of the matrix of the blocked Gauss-Jordan: GM = false, the swizzled shared-memory
+// layout above (16 <= N <= 120 in FP64); GM = true, column-major in the block's slot of a
+// global workspace (120 < N <= 256: the working set of the concurrent blocks stays largely in
+// L2, and every access of the update is a 128-byte run of 8 consecutive rows).
+template <bool GM> __device__ __forceinline__ int bix(int i, int j, int N) { return GM ? i + j * N : swz(i, j, N); }
+// panel warps: one thread per row
+template <bool GM> __host__ __device__ __forceinline__ int bgj_pw(int N) { return GM ? (N + 31) / 32 : 4; }
+constexpr int BGJ_MAXN_GM = 256;
+
+// Blocked Gauss-Jordan inversion with the matrix in (swizzled) shared memory (GM = false,
+// 16 <= N <= 120) or in a global workspace (GM = true, 120 < N <= 256). Per panel
+// K = [k0, k0 + 16):
+//   panel   the panel warps (4, or ceil(N/32) <= 8), thread i holding row i of the panel
+//           columns in registers: per column
 //           k the pivot search, the exchange of rows k and p (the panel part through shared
 //           memory, the rest of the two rows in place), and the elimination restricted to
 //           the panel columns; two 128-thread barriers per column
@@ -232,25 +243,29 @@ __device__ __forceinline__ void warp_argmax_all(double &v, int &i) {
 //           tensor cores; the warp reads its A[K, j] fragment before it rewrites those rows,
 //           so no block barrier separates the two
 // The row interchanges are undone by column interchanges in reverse order at the end.
-__global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
+template <bool GM>
+__global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj_t(DysonArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int PWM = GM ? 8 : 4;  // panel warps at most
     const int N = a.N;
-    zc *M = (zc *)smem_raw;
-    // static shared memory stays below 1536 bytes (use_blocked): N = 120 takes the rest
-    __shared__ unsigned char perm[128];
-    __shared__ unsigned long long cand_k[4];  // each panel warp's pivot key (0: no row searched)
-    __shared__ int cand_i[4];
-    __shared__ zc cand_row[4][GJ_B];  // each panel warp's pivot candidate row (panel part)
-    __shared__ zc krow[GJ_B];         // the panel part of row k before the exchange
+    zc *M = GM ? a.ws + (size_t)blockIdx.x * N * N : (zc *)smem_raw;
+    // static shared memory of the shared-memory form stays below 1536 bytes (use_blocked):
+    // N = 120 takes the rest
+    __shared__ unsigned char perm[GM ? BGJ_MAXN_GM : 128];
+    __shared__ unsigned long long cand_k[PWM];  // each panel warp's pivot key (0: no row searched)
+    __shared__ int cand_i[PWM];
+    __shared__ zc cand_row[PWM][GJ_B];  // each panel warp's pivot candidate row (panel part)
+    __shared__ zc krow[GJ_B];           // the panel part of row k before the exchange
     __shared__ int first_zero_s;
     const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const int g = lane >> 2, t4 = lane & 3;
     const int mtiles = (N + 15) / 16, ntiles = (N + 7) / 8;
+    const int npw = bgj_pw<GM>(N);  // panel warps
 
     for (int iw = a.iw0 + blockIdx.x; iw < a.iw1; iw += gridDim.x) {
         if (a.Ain) {
             const zc *A = a.Ain + (size_t)(iw - a.iw0) * N * N;
-            for (int idx = tid; idx < N * N; idx += nthr) M[swz(idx % N, idx / N, N)] = A[idx];
+            for (int idx = tid; idx < N * N; idx += nthr) M[bix<GM>(idx % N, idx / N, N)] = A[idx];
         } else {
             const double w = a.omega[iw];
             const zc *SR = a.SigR + (size_t)iw * a.nA * a.nA;
@@ -267,7 +282,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                     }
                 }
                 if (i == j) v.x += w;
-                M[swz(i, j, N)] = v;
+                M[bix<GM>(i, j, N)] = v;
             }
         }
         if (tid == 0) first_zero_s = 0;
@@ -276,13 +291,13 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
         for (int k0 = 0; k0 < N; k0 += GJ_B) {
             const int kb = min(GJ_B, N - k0);
             // ---- panel
-            if (warp < 4) {
+            if (warp < npw) {
                 const int i = tid;  // this thread's row
                 // R[j] holds panel column (c + j) mod 16 at step c: the current column is always
                 // R[0] and the step loop need not be unrolled (padding columns stay zero)
                 zc R[GJ_B];
 #pragma unroll
-                for (int c = 0; c < GJ_B; c++) R[c] = (i < N && c < kb) ? M[swz(i, k0 + c, N)] : zc{0, 0};
+                for (int c = 0; c < GJ_B; c++) R[c] = (i < N && c < kb) ? M[bix<GM>(i, k0 + c, N)] : zc{0, 0};
 #pragma unroll 1
                 for (int c = 0; c < kb; c++) {
                     const int k = k0 + c;
@@ -320,13 +335,12 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                         for (int j = 0; j < GJ_B; j++) krow[j] = R[j];
                     }
-                    panel_bar();
+                    panel_bar(32 * npw);
                     // the largest key; on a tie the lower warp (lower rows) wins, as the first
                     // maximum. The warp holding row k has a key > 0, so p is a row in [k, N).
                     unsigned long long bk = cand_k[0];
                     int wb = 0;
-#pragma unroll
-                    for (int q = 1; q < 4; q++) {
+                    for (int q = 1; q < npw; q++) {
                         const unsigned long long ck = cand_k[q];
                         if (ck > bk) {
                             bk = ck;
@@ -370,18 +384,18 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                     // the rest of rows k and p (thread i moves column i, its own earlier
                     // exchanges first)
                     if (p != k && i < N && (i < k0 || i >= k0 + kb)) {
-                        zc tt = M[swz(k, i, N)];
-                        M[swz(k, i, N)] = M[swz(p, i, N)];
-                        M[swz(p, i, N)] = tt;
+                        zc tt = M[bix<GM>(k, i, N)];
+                        M[bix<GM>(k, i, N)] = M[bix<GM>(p, i, N)];
+                        M[bix<GM>(p, i, N)] = tt;
                     }
-                    panel_bar();  // cand_row and krow are rewritten by the next column
+                    panel_bar(32 * npw);  // cand_row and krow are rewritten by the next column
                 }
                 // after kb steps R[j] holds column (kb + j) mod 16
                 if (i < N) {
 #pragma unroll
                     for (int j = 0; j < GJ_B; j++) {
                         const int c = (kb + j) & (GJ_B - 1);
-                        if (c < kb) M[swz(i, k0 + c, N)] = R[j];
+                        if (c < kb) M[bix<GM>(i, k0 + c, N)] = R[j];
                     }
                 }
             }
@@ -394,7 +408,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int kr = t4 + 4 * q, c = j0 + g;
-                    zc v = (kr < kb && c < N) ? M[swz(k0 + kr, c, N)] : zc{0, 0};
+                    zc v = (kr < kb && c < N) ? M[bix<GM>(k0 + kr, c, N)] : zc{0, 0};
                     br[q] = v.x;
                     bi[q] = v.y;
                 }
@@ -406,7 +420,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                     for (int q = 0; q < 8; q++) {
                         const int r = i0 + g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
-                        zc v = (r < N && c < kb) ? M[swz(r, k0 + c, N)] : zc{0, 0};
+                        zc v = (r < N && c < kb) ? M[bix<GM>(r, k0 + c, N)] : zc{0, 0};
                         ar[q] = v.x;
                         ai[q] = v.y;
                     }
@@ -415,7 +429,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
                     for (int q = 0; q < 4; q++) {
                         const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
                         own[q] = r < N && c < N && (r < k0 || r >= k0 + kb) && (c < k0 || c >= k0 + kb);
-                        zc v = own[q] ? M[swz(r, c, N)] : zc{0, 0};
+                        zc v = own[q] ? M[bix<GM>(r, c, N)] : zc{0, 0};
                         cr[q] = v.x;
                         ci[q] = v.y;
                     }
@@ -423,7 +437,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
                         const int r = i0 + g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
-                        if (own[q]) M[swz(r, c, N)] = zc{cr[q], ci[q]};
+                        if (own[q]) M[bix<GM>(r, c, N)] = zc{cr[q], ci[q]};
                     }
                 }
                 // the pivot rows
@@ -431,7 +445,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                 for (int q = 0; q < 8; q++) {
                     const int r = g + 8 * (q & 1), c = t4 + 4 * (q >> 1);
-                    zc v = (r < kb && c < kb) ? M[swz(k0 + r, k0 + c, N)] : zc{0, 0};
+                    zc v = (r < kb && c < kb) ? M[bix<GM>(k0 + r, k0 + c, N)] : zc{0, 0};
                     ar[q] = v.x;
                     ai[q] = v.y;
                 }
@@ -439,7 +453,7 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     const int r = g + 8 * (q >> 1), c = j0 + 2 * t4 + (q & 1);
-                    if (r < kb && c < N && (c < k0 || c >= k0 + kb)) M[swz(k0 + r, c, N)] = zc{cr[q], ci[q]};
+                    if (r < kb && c < N && (c < k0 || c >= k0 + kb)) M[bix<GM>(k0 + r, c, N)] = zc{cr[q], ci[q]};
                 }
             }
             __syncthreads();
@@ -449,9 +463,9 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
             for (int k = N - 1; k >= 0; k--) {
                 int p = perm[k];
                 if (p != k) {
-                    zc tt = M[swz(tid, k, N)];
-                    M[swz(tid, k, N)] = M[swz(tid, p, N)];
-                    M[swz(tid, p, N)] = tt;
+                    zc tt = M[bix<GM>(tid, k, N)];
+                    M[bix<GM>(tid, k, N)] = M[bix<GM>(tid, p, N)];
+                    M[bix<GM>(tid, p, N)] = tt;
                 }
             }
         }
@@ -465,11 +479,11 @@ __global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj(DysonArgs a) {
             zc *G = a.Gout + (size_t)iw * nA * nA;
             for (int idx = tid; idx < nA * nA; idx += nthr) {
                 int p = idx % nA, q = idx / nA;
-                G[idx] = M[swz(a.act[p], a.act[q], N)];
+                G[idx] = M[bix<GM>(a.act[p], a.act[q], N)];
             }
         } else {
             zc *G = a.Gout + (size_t)(iw - a.iw0) * N * N;
-            for (int idx = tid; idx < N * N; idx += nthr) G[idx] = M[swz(idx % N, idx / N, N)];
+            for (int idx = tid; idx < N * N; idx += nthr) G[idx] = M[bix<GM>(idx % N, idx / N, N)];
         }
         __syncthreads();
     }
@@ -1062,9 +1076,23 @@ static size_t dyson_smem(int N) { return sizeof(zc) * (size_t)N * N; }
 static bool dyson_fits(int N) { return dyson_fits_smem(N); }
 
 static bool use_blocked(int N) { return N >= 16 && N <= 128 && (size_t)swz_units(N) * 16 + 1536 <= (size_t)SMEM_MAX; }
+// the blocked kernel with the matrix in the global workspace: orders above the shared-memory
+// limit up to 256
+static bool use_blocked_gm(int N) { return !use_blocked(N) && N > 16 && N <= BGJ_MAXN_GM; }
+static inline auto dyson_bgj = dyson_bgj_t<false>;
 
 static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks, int variant) {
     const int N = a.N;
+    if (variant == DYSON_BLOCKED && use_blocked_gm(N) && h->d_Gws) {
+        // one block per SM: the concurrent matrices (148 x N^2 x 16 B) stay mostly in L2
+        a.ws = h->d_Gws;
+        nblocks = std::min<int>(std::min(nblocks, 148), (int)h->ws_slots);
+        int pi = prof_begin(h, K_DYSON);
+        dyson_bgj_t<true><<<nblocks, BGJ_THREADS, 0, h->stream>>>(a);
+        prof_end(h, pi);
+        QS_CUDA(h, cudaGetLastError());
+        return 0;
+    }
     if (variant == DYSON_BLOCKED && use_blocked(N)) {
         size_t sm = (size_t)swz_units(N) * sizeof(zc);
         QS_CUDA(h, smem_cap((const void *)dyson_bgj));
@@ -1112,6 +1140,14 @@ int invert_batched_dev(cudaStream_t st, int N, int batch, zc *d_A, int *d_info, 
         count_launch();
         dyson_bgj<<<nb, BGJ_THREADS, sm, st>>>(a);
         e = cudaGetLastError();
+        return e == cudaSuccess ? 0 : -(int)e;
+    }
+    if (use_blocked_gm(N) && d_ws && ws_slots > 0) {
+        a.ws = d_ws;
+        nb = std::min(std::min(nb, 148), ws_slots);
+        count_launch();
+        dyson_bgj_t<true><<<nb, BGJ_THREADS, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
         return e == cudaSuccess ? 0 : -(int)e;
     }
     if (dyson_fits(N)) {
@@ -1175,7 +1211,7 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         a.Gout = h->d_G;
         {
             const int cand[2] = {DYSON_BLOCKED, DYSON_UNBLOCKED};
-            const bool two = use_blocked(N);
+            const bool two = use_blocked(N) || (use_blocked_gm(N) && h->d_Gws);
             rc = tune_launch(h, TUNE_DYSON, tune_key(N, n), two ? cand : cand + 1, two ? 2 : 1, DYSON_BLOCKED,
                              [&](int v) { return launch_dyson(h, a, std::min(n, 148 * 16), v); });
             if (rc) return rc;

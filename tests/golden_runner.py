@@ -12,12 +12,13 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
+GOLDEN_SANCHO = os.path.join(GOLDEN, "sancho")  # SANCHO's suite (SANCHO/tests), same runner and tolerances
 TOL_ABS, TOL_REL = 1e-6, 1e-5
 
 
-def cases():
+def cases(root=GOLDEN):
     out = []
-    for line in open(os.path.join(GOLDEN, "cases.txt")):
+    for line in open(os.path.join(root, "cases.txt")):
         line = line.strip()
         if not line or line.startswith("#"):
             continue
@@ -65,9 +66,9 @@ def compare_files(new, ref, ta=TOL_ABS, tr=TOL_REL):
     return (not bad), worst, "; ".join(bad[:3])
 
 
-def run_case(exe, case, workroot, env=None, timeout=600):
+def run_case(exe, case, workroot, env=None, timeout=600, root=GOLDEN):
     """Copy the case, run `exe` in it. Returns (exit code, work dir)."""
-    src = os.path.join(GOLDEN, "cases", case)
+    src = os.path.join(root, "cases", case)
     work = os.path.join(workroot, case)
     if os.path.isdir(work):
         shutil.rmtree(work)
@@ -84,15 +85,15 @@ def run_case(exe, case, workroot, env=None, timeout=600):
     return r.returncode, work
 
 
-def check_case(exe, case, rc_expected, refs, workroot, env=None):
-    rc, work = run_case(exe, case, workroot, env)
+def check_case(exe, case, rc_expected, refs, workroot, env=None, root=GOLDEN):
+    rc, work = run_case(exe, case, workroot, env, root=root)
     msgs = []
     ok = rc == rc_expected
     if not ok:
         msgs.append(f"exit code {rc}, expected {rc_expected} (see {work}/stdout.txt)")
     worst = {}
     for r in refs:
-        good, w, m = compare_files(os.path.join(work, r), os.path.join(GOLDEN, "cases", case, "reference", r))
+        good, w, m = compare_files(os.path.join(work, r), os.path.join(root, "cases", case, "reference", r))
         worst[r] = w
         if not good:
             ok = False

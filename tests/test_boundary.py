@@ -1,5 +1,5 @@
 """The drop-in boundary: the C-ABI library loads and exports every entry point that
-include/qsb200.h declares (no GPU work here)."""
+include/qsb200.h and include/qsa200.h declare (no GPU work here)."""
 import ctypes
 import os
 import re
@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared(header):
     text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(qsh?_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(qs[ha]?h?_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_cuda_library_exports_every_declared_entry_point():
@@ -26,15 +26,29 @@ def test_cuda_library_exports_every_declared_entry_point():
     assert set(qb.C_ABI) <= set(names)
 
 
+def test_cuda_library_exports_every_sancho_entry_point():
+    import sancho_b200 as sb
+    lib = ctypes.CDLL(qb.LIB_PATH)
+    names = [n for n in declared("qsa200.h") if n.startswith("qsa_")]
+    assert len(names) == 10
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(sb.C_ABI) == set(names)
+
+
 def test_host_library_exports_every_declared_entry_point():
     lib = ctypes.CDLL(qb.HOST_PATH)
     names = [n for n in declared("qs_host.h") if n.startswith("qsh_")]
+    names += [n for n in declared("qsa_host.h") if n.startswith("qsah_")]
+    assert any(n.startswith("qsah_") for n in names)
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 
 
-def test_program_binary_is_built():
+def test_program_binaries_are_built():
+    import sancho_b200 as sb
     assert os.access(qb.PROGRAM, os.X_OK)
+    assert os.access(sb.PROGRAM, os.X_OK)
 
 
 def test_memory_estimate_grows_with_the_problem_and_needs_no_device():
@@ -64,6 +78,8 @@ C_CLIENT = r"""
 #include <string.h>
 #include "qsb200.h"
 #include "qs_host.h"
+#include "qsa200.h"
+#include "qsa_host.h"
 
 int main(void) {
     void *table[] = {
@@ -108,6 +124,7 @@ def test_headers_are_plain_c_and_link(tmp_path):
     if not cc:
         pytest.skip("no C compiler")
     names = declared("qsb200.h") + [n for n in declared("qs_host.h") if n.startswith("qsh_")]
+    names += declared("qsa200.h") + [n for n in declared("qsa_host.h") if n.startswith("qsah_")]
     src = tmp_path / "client.c"
     src.write_text(C_CLIENT.replace("%TABLE%", ",\n".join(f"        (void *)&{n}" for n in names)))
     exe = tmp_path / "client"

@@ -17,7 +17,7 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
-@pytest.mark.parametrize("N", [1, 2, 5, 8, 16, 18, 24, 33, 64, 100, 120, 121, 128, 200])
+@pytest.mark.parametrize("N", [1, 2, 5, 8, 16, 18, 24, 33, 64, 100, 120, 121, 128, 136, 192, 200, 248, 256])
 def test_invert_batched_matches_numpy(N):
     rng = np.random.default_rng(N)
     batch = 37
@@ -269,6 +269,28 @@ def test_forced_kernel_variants_match_oracle(mode, ions_turns):
     try:
         gs, os_ = qb.Solver(m), oracle_lib.solver(m)
         x = os_.initial_vector(0.2) + 1e-3 * np.random.default_rng(5).standard_normal(gs.n_vec)
+        Fg, _ = gs.residual(0.2, x)
+        Fo, _ = os_.residual(0.2, x)
+        assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
+    finally:
+        qb.autotune(1)
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("ions_turns", [(17, 4), (16, 6)])
+def test_dyson_above_shared_memory_matches_oracle(mode, ions_turns):
+    """N = 136, 192: the matrix no longer fits in shared memory. Mode 2 forces the blocked
+    tensor-core Gauss-Jordan on the global workspace, mode 3 the unblocked one; the residual
+    within 1e-11 of the oracle either way."""
+    ni, nt = ions_turns
+    m = qb.Model.helix(N_ions=ni, N_turns=nt, hel_length=0.34 * nt, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
+                       lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
+                       dw=1.0, up=1.0, delta=0.08, order=2)
+    qb.autotune(mode)
+    try:
+        gs, os_ = qb.Solver(m), oracle_lib.solver(m)
+        assert gs.nA == 2 * ni * nt
+        x = os_.initial_vector(0.2) + 1e-3 * np.random.default_rng(8).standard_normal(gs.n_vec)
         Fg, _ = gs.residual(0.2, x)
         Fo, _ = os_.residual(0.2, x)
         assert np.max(np.abs(Fg - Fo)) < 1e-11 * max(1.0, np.max(np.abs(x)))
