@@ -13,10 +13,11 @@ continuation from the previous one, then Current and the observables):
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--precision both|fp64|mixed]
                   [--serve R] [--serve-rate r] [--serve-inflight k]
 
-Default: the FP64 form, then the mixed form (the headline value), their ratio and the
-error of every observable of the mixed form against the FP64 one over the points both
-converged; the CPU oracle on a bounded sample of the same sweep beside the GPU on the same
-sample; then a serving stream (p50/p99 latency of IV-point requests through qs_server).
+Default: the FP64 form (the headline value), then the mixed form beside it with its ratio
+and the error of every observable against the FP64 one over the points both converged;
+the CPU oracle on a bounded sample of the same sweep; then a serving stream (p50/p99
+latency of IV-point requests through qs_server). --case sancho / cfg2 / cfg4 run the other
+workloads (their lines name them).
 
 N > 1 (launched with torch.distributed.run): replicas. Rank r solves its own contiguous
 block of the voltage sweep; no data-path collective. value = all IV points / max over
@@ -156,7 +157,7 @@ def bench_config(n_omega, ions, turns, nhist, world):
                         "with continuation; the first W voltages warm up, the next K are timed",
             "broyden": {"alpha_mix": b["alpha_mix"], "nhist": b["nhist"], "history": "single" if b["single_history"]
                         else "double", "tolf": b["tolf"], "maxscf": b["maxscf"]},
-            "forms": "FP64 GPU form, then the mixed form (headline)",
+            "forms": "FP64 GPU form (headline), then the mixed form (under \"mixed\")",
             "parallelism": f"replicas x{world}", "l2": "working set ~147 GB >> L2 126 MB (no flush needed)"}
 
 
@@ -563,6 +564,93 @@ def run_case(args, device):
     return 0
 
 
+SANCHO_CHAIN = dict(N_sites=10, E_CC=2.0, t_hop=-0.4, U_int=0.8, GammaL=1.0, GammaR=1.0, T=300.0, mu=2.0, dw=1.0,
+                    up=1.0, delta=0.002, order=3)
+SANCHO_VOLTS = [-0.5, -0.25, 0.0, 0.25, 0.5]
+
+
+def sancho_input(path, chain, volts):
+    """SANCHO's input.dat for the chain (the keys of SANCHO/src/input_output.f90:28-104) and
+    the voltage sweep volts[0] .. volts[-1]"""
+    os.makedirs(path, exist_ok=True)
+    keys = dict(chain, V=volts[0], Vf=volts[-1], delv=volts[1] - volts[0], alpha_mix=0.3, nhist=8, maxscf=200,
+                tolf=1e-6)
+    with open(os.path.join(path, "input.dat"), "w") as f:
+        for k, v in keys.items():
+            f.write(f"{k} = {v}\n")
+    return path
+
+
+def run_sancho(args, device):
+    """--case sancho: SANCHO's order-3 chain (10 sites, 1740 energies; SANCHO's regression case
+    scaled up: the same chain and settings, a finer grid and more sites) swept over five
+    voltages with continuation on the B200 solver (include/qsa200.h), its kernel families
+    against the FP64 roofline, and the CPU oracle's time per SCF iteration of the same sweep."""
+    import tempfile
+
+    import quichotte_b200 as qb
+    import sancho_b200 as sb
+    d = sancho_input(tempfile.mkdtemp(prefix="qs_sancho_"), SANCHO_CHAIN, SANCHO_VOLTS)
+    m = sb.SanchoModel.load(d)
+    s = sb.SanchoSolver(m, device=device)
+    # warm-up: one fresh solve (module load, first launches)
+    s.solve_scf(SANCHO_VOLTS[0], True)
+    s.profile(True)
+    l0 = qb.kernel_launches()
+    pts, ok, wall = [], False, 0.0
+    for k, V in enumerate(SANCHO_VOLTS):
+        t = time.perf_counter()
+        r = s.solve_scf(V, k == 0 or not ok)
+        J = s.current(V)
+        s.observables()
+        wall += time.perf_counter() - t
+        ok = r["converged"]
+        pts.append(dict(V=V, converged=ok, n_iter=r["n_iter"], J=J))
+    prof = s.profile(False)
+    launches = qb.kernel_launches() - l0
+    n_it = sum(p["n_iter"] for p in pts)
+    conv = sum(int(p["converged"]) for p in pts)
+    Na, n = m.N_sites, m.n_omega
+    # algorithmic FP64 work per SCF iteration of the direct sums (complex MAC = 8 flops):
+    # chi and phi 6 MACs per (element, output, summand) over n^2 (output, summand) pairs each,
+    # the particle-hole and particle-particle convolutions 3 MACs each
+    fl_bub = 2 * 6 * 8 * Na * Na * n * n
+    fl_sig = 2 * 3 * 8 * Na * Na * n * n
+    ms_bub, ms_sig = prof["bubbles"][0], prof["sigma"][0]
+    peak = 37.0  # TFLOP/s, B200 FP64 (nominal; the measured peaks hold no FP64 figure)
+    achieved = fl_bub * n_it / (ms_bub * 1e-3) / 1e12 if ms_bub > 0 else 0.0
+    # CPU: the oracle's time per SCF iteration (one residual of the same chain at the first voltage)
+    cpu = {}
+    if not args.no_cpu_baseline:
+        op = _oracle(os.cpu_count())
+        om = op.SanchoChain(**SANCHO_CHAIN)
+        o = op.SanchoSolver(om)
+        x = o.initial_vector(SANCHO_VOLTS[0])
+        t = time.perf_counter()
+        o.residual(SANCHO_VOLTS[0], x)
+        t_it = time.perf_counter() - t
+        cpu = {"value": conv / (t_it * n_it) if t_it > 0 else 0.0, "unit": "IV points/s", "cores": os.cpu_count(),
+               "kind": "port", "seconds_per_scf_iteration": t_it,
+               "sample": f"one scf_residual of the same chain (OpenMP over elements) x {n_it} SCF iterations "
+                         "the B200 sweep took"}
+    line = {"metric": "converged IV points/s", "value": conv / wall if wall > 0 else 0.0, "unit": "IV points/s",
+            "n_gpus": 1, "steps": len(SANCHO_VOLTS), "warmup": 1, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "case": "sancho",
+            "config": {"workload": f"SANCHO chain, {Na} sites, order 3, {n} energies (delta 0.002 eV), U 0.8 eV, "
+                                   "E_CC 2 eV, t -0.4 eV, Gamma 1 eV, T 300 K, mu 2 eV; V -0.5..0.5 step 0.25 with "
+                                   "continuation; alpha_mix 0.3, nhist 8, tolf 1e-6 (SANCHO's defaults)"},
+            "scf_iterations": [p["n_iter"] for p in pts], "converged": [p["converged"] for p in pts],
+            "currents": [p["J"] for p in pts], "seconds_per_scf_iteration": wall / max(n_it, 1),
+            "kernel_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1]}, "gpu_launches": launches,
+            "roofline": {"kernel": "sa_bubbles (chi + phi)", "bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "peak_kind": "nominal",
+                         "flop_per_iteration": fl_bub,
+                         "sigma_tflops": fl_sig * n_it / (ms_sig * 1e-3) / 1e12 if ms_sig > 0 else 0.0},
+            "cpu_baseline": cpu}
+    print(json.dumps(finite(line), allow_nan=False), flush=True)
+    return 0
+
+
 def setup_timing(qb, m, repeats=3):
     """The set-up's dense linear algebra on the device, through the public entry points with
     host arrays (copies included), beside LAPACK through numpy on the host cores: the grid
@@ -681,13 +769,14 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-inflight", type=int, default=4, help="solves on the device at once")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
-                    help="both: the FP64 form, then the mixed form (headline value), with their ratio")
+                    help="both: the FP64 form (headline value), then the mixed form, with their ratio")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving stream (--serve requests at --serve-rate), FP64 then mixed, and print "
                          "its line")
-    ap.add_argument("--case", default="cfg1", choices=["cfg1", "cfg2", "cfg4"],
+    ap.add_argument("--case", default="cfg1", choices=["cfg1", "cfg2", "cfg4", "sancho"],
                     help="cfg1: the workload above (default); cfg2 / cfg4: the multi-orbital molecule and the "
-                         "256-state helix at the reduced sizes one B200 holds (their line names the deviation)")
+                         "256-state helix at the reduced sizes one B200 holds (their line names the deviation); "
+                         "sancho: SANCHO's order-3 chain on the B200 SANCHO solver")
     ap.add_argument("--setup-scan", action="store_true",
                     help="time the device set-up (eigenproblem, Loewdin) over sizes against LAPACK, print, exit")
     args = ap.parse_args()
@@ -701,6 +790,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.case == "sancho":
+        return run_sancho(args, local)
     if args.case != "cfg1":
         return run_case(args, local)
     if args.serve_only:
@@ -778,8 +869,10 @@ def main():
     arms = {}
     for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
         arms[prec] = run_arm(qb.QS_PREC_MIXED if prec == "mixed" else qb.QS_PREC_FP64)
-    head = arms.get("mixed") or arms["fp64"]
+    # the headline is the FP64 form (the reference's arithmetic); the mixed form stands beside it
+    head = arms.get("fp64") or arms["mixed"]
     f64 = arms.get("fp64")
+    mix = arms.get("mixed")
     dev_s, wall, n_conv = head["dev_s"], head["wall"], head["n_conv"]
     launches, clk = head["launches"], head["clk"]
     prof = (f64 or head)["prof"]
@@ -821,7 +914,7 @@ def main():
                     "traffic_note": "DRAM bytes per launch from an ncu capture, scaled per unit" if tpu else None,
                     "peak_source": src_note,
                     "per_launch_work": per_launch, "launches": cnt, "avg_launch_ms": ms / cnt}
-        prec_name = "mixed" if "mixed" in arms else "fp64"
+        prec_name = "fp64" if f64 is not None else "mixed"
         pts = head["points"]
         line = {
             "metric": "converged IV points/s", "value": n_conv / dev_s if dev_s > 0 else 0.0,
@@ -842,19 +935,20 @@ def main():
             "clocks": clk,
             "currents_A": [list(p["J"]) for p in pts],
         }
-        if "mixed" in arms:
-            line["mixed_form"] = ("Sigma2 FFTs, 2x2 algebra and spectra in FP32 while max|F| > max(1e-5, 100 tolf) "
-                                  "(the FP32 noise floor is ~1e-5); then FP64 steps until an FP64 residual meets "
-                                  "tolf; Dyson/Keldysh, Broyden and observables FP64")
-            line["fp32_steps_per_point"] = [p["n_mixed"] for p in pts]
-        if f64 is not None and "mixed" in arms:
-            line["fp64"] = {"value": f64["value"], "e2e": f64["e2e"], "ms_per_step": 1000.0 * f64["dev_s"] / args.steps,
-                            "converged": [bool(p["converged"]) for p in f64["points"]],
-                            "scf_steps_per_point": [p["n_iter"] for p in f64["points"]],
-                            "kernel_ms": {k: round(v[0], 3) for k, v in f64["prof"].items() if v[1]}}
-            line["mixed_over_fp64"] = head["value"] / f64["value"] if f64["value"] > 0 else None
-            line["err_vs_fp64"] = observable_errors(f64["points"], pts)
-            line["kernel_ms_mixed"] = {k: round(v[0], 3) for k, v in head["prof"].items() if v[1]}
+        if mix is not None and f64 is not None:
+            line["mixed"] = {
+                "form": ("Sigma2 FFTs, 2x2 algebra and spectra in FP32, and the Keldysh products on the fastest of "
+                         "the 3xTF32 tensor-core kernel and the FP64 ones (autotuned), while max|F| is above "
+                         "max(1e-5, 100 tolf) and still falling; then FP64 steps until an FP64 residual meets tolf; "
+                         "Dyson, Broyden and observables FP64"),
+                "value": mix["value"], "e2e": mix["e2e"], "ms_per_step": 1000.0 * mix["dev_s"] / args.steps,
+                "converged": [bool(p["converged"]) for p in mix["points"]],
+                "scf_steps_per_point": [p["n_iter"] for p in mix["points"]],
+                "fp32_steps_per_point": [p["n_mixed"] for p in mix["points"]],
+                "kernel_ms": {k: round(v[0], 3) for k, v in mix["prof"].items() if v[1]},
+                "clocks": mix["clk"], "gpu_launches": mix["launches"],
+                "over_fp64": mix["value"] / f64["value"] if f64["value"] > 0 else None,
+                "err_vs_fp64": observable_errors(f64["points"], mix["points"])}
         if world == 1 and args.serve > 0:
             line["serving"] = run_serving(qb, args.serve, args.serve_rate, args.serve_inflight, qb.QS_PREC_FP64)
             line["serving"]["workload"] = (f"serving stream, first {args.serve} of the seeded 512-request stream: random "

@@ -71,6 +71,13 @@ int qsa_residual(qsa_handle *h, double Volt, const double *x, double *F, int *ab
 int qsa_self_energies(qsa_handle *h, const double *x, double *Sig2R, double *Sig2L, double *Sig3R,
                       double *Sig3L);
 
+/* Extension (no counterpart in SANCHO): per-family device time in ms and launch counts since
+ * the last call, as qs_profile (enable 1/0 switches event timing on/off, -1 only reads).
+ * Families: 0 Dyson (W build + inversion), 1 Keldysh (products + pack), 2 bubbles chi/phi,
+ * 3 order-3 products D/E, 4 self-energy convolutions, 5 (unused), 6 Broyden, 7 reductions,
+ * 8 other. Returns the number of families. */
+int qsa_profile(qsa_handle *h, int enable, double *ms, int64_t *launches, int nfam);
+
 #ifdef __cplusplus
 }
 #endif

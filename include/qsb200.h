@@ -225,11 +225,13 @@ void qs_server_destroy(qs_server *s);
  * Kernel variants whose relative speed depends on the size (kind 0: Dyson, blocked tensor-
  * core or unblocked Gauss-Jordan; kind 1: Keldysh, tensor-core or CUDA-core GEMMs; kinds 2
  * and 3: the tile width 4 or 2 of the persistent Sigma2 kernels A and C, +2^20 in the key
- * for the FP32 ones) are timed on the first launch at a new size and the fastest is kept
- * for the process.
+ * for the FP32 ones; kind 4: the Keldysh step of a mixed solve's FP32 phase, variant 3 the
+ * 3xTF32 kernel on the fifth-generation tensor cores, 1 / 2 the FP64 ones) are timed on the
+ * first launch at a new size and the fastest is kept for the process.
  * qs_autotune(1) tunes (default), qs_autotune(0) uses the size heuristics only, 2 / 3 force
- * variant 1 (tensor-core / blocked) / 2 wherever it applies, qs_autotune(-1) forgets the
- * recorded choices. qs_tuned_choice returns the recorded variant (1 or 2) or -1; a decision
+ * the first (kind 4: the 3xTF32 kernel; else the tensor-core / blocked variant) / last
+ * applicable variant, qs_autotune(-1) forgets the recorded choices. qs_tuned_choice returns
+ * the recorded variant (1, 2 or 3) or -1; a decision
  * is keyed by size = order + 1024 * floor(log2(n_omega)) (order N for Dyson, nA for Keldysh). */
 int qs_autotune(int mode);
 int qs_tuned_choice(int kind, int size);

@@ -217,3 +217,104 @@ class Solver:
 
     def __del__(self):
         self.close()
+
+
+# ---- SANCHO (the spinless chain; paths relative to the reference project's SANCHO/) ----
+
+class SanchoChain:
+    """The chain model of SANCHO's input (SANCHO/src/hamiltonian.f90:35-137: E_CC on the
+    diagonal, t_hop between neighbours; leads GammaL on site 1 and GammaR on the last site;
+    uniform U, SANCHO/src/input_output.f90:106-132) and its grid (SANCHO/src/sancho.f90:
+    58-92: w_init = min eig(H) - dw, n = int((max eig(H) + up - w_init)/delta),
+    omega_i = w_init + i delta)."""
+
+    def __init__(self, N_sites, E_CC, t_hop, U_int, GammaL, GammaR, T, mu, dw, up, delta, order):
+        n = N_sites
+        H = np.zeros((n, n), np.complex128)
+        for i in range(n):
+            H[i, i] = E_CC
+            if i + 1 < n:
+                H[i, i + 1] = H[i + 1, i] = t_hop
+        self.N_sites, self.order, self.H = n, order, np.asfortranarray(H)
+        self.GammaL = np.zeros((n, n), np.complex128, order="F")
+        self.GammaR = np.zeros((n, n), np.complex128, order="F")
+        self.GammaL[0, 0] = GammaL
+        self.GammaR[n - 1, n - 1] = GammaR
+        self.U_site = np.full(n, float(U_int))
+        ev = np.linalg.eigvalsh(H)
+        w_init, w_fin = ev[0] - dw, ev[-1] + up
+        self.n_omega = int((w_fin - w_init) / delta)
+        self.omega = w_init + delta * np.arange(1, self.n_omega + 1)
+        self.mu, self.beta, self.delta = mu, 1.0 / (KB * T), delta
+
+
+class _SanchoProblem(ctypes.Structure):
+    """qsa_problem of include/qsa200.h."""
+    _fields_ = ([(k, ctypes.c_int) for k in ("N_sites", "order", "n_omega")]
+                + [(k, ctypes.c_void_p) for k in ("H", "GammaL", "GammaR", "U_site", "omega")]
+                + [(k, ctypes.c_double) for k in ("mu", "beta", "delta", "alpha_mix", "tolf")]
+                + [(k, ctypes.c_int) for k in ("nhist", "maxscf", "device")])
+
+
+class SanchoSolver:
+    """One SANCHO oracle solver (qsao_create ... qsao_destroy)."""
+
+    def __init__(self, model, alpha_mix=0.3, nhist=8, tolf=1e-6, maxscf=200):
+        L = lib()
+        for name, args, res in (("qsao_create", [ctypes.POINTER(_SanchoProblem), ctypes.POINTER(ctypes.c_void_p)], None),
+                                ("qsao_destroy", [ctypes.c_void_p], "void"),
+                                ("qsao_vector_length", [ctypes.c_void_p], ctypes.c_int64),
+                                ("qsao_solve_scf", [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                                    ctypes.POINTER(_Result)], None),
+                                ("qsao_residual", [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.POINTER(ctypes.c_int)], None),
+                                ("qsao_initial_vector", [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p], None)):
+            f = getattr(L, name)
+            f.argtypes = args
+            if res == "void":
+                f.restype = None
+            elif res is not None:
+                f.restype = res
+        m = model
+        self._keep = [np.asfortranarray(m.H), np.asfortranarray(m.GammaL), np.asfortranarray(m.GammaR),
+                      np.ascontiguousarray(m.U_site, np.float64), np.ascontiguousarray(m.omega, np.float64)]
+        ptr = [a.ctypes.data_as(ctypes.c_void_p) for a in self._keep]
+        self._p = _SanchoProblem(m.N_sites, m.order, m.n_omega, *ptr, m.mu, m.beta, m.delta, alpha_mix, tolf, nhist,
+                                 maxscf, 0)
+        self.maxscf = maxscf
+        self._h = ctypes.c_void_p()
+        if L.qsao_create(ctypes.byref(self._p), ctypes.byref(self._h)) != 0:
+            raise RuntimeError("qsao_create failed")
+        self.n_vec = int(L.qsao_vector_length(self._h))
+
+    def solve_scf(self, V, fresh_start=True):
+        cap = self.maxscf + 2
+        log = (_Step * cap)()
+        r = _Result()
+        r.log, r.log_cap = log, cap
+        t = time.perf_counter()
+        rc = lib().qsao_solve_scf(self._h, V, int(fresh_start), ctypes.byref(r))
+        if rc != 0:
+            raise RuntimeError(f"qsao_solve_scf failed ({rc})")
+        return {"converged": bool(r.converged), "n_iter": r.n_iter, "wall": time.perf_counter() - t}
+
+    def initial_vector(self, V):
+        x = np.zeros(self.n_vec)
+        lib().qsao_initial_vector(self._h, V, x.ctypes.data_as(ctypes.c_void_p))
+        return x
+
+    def residual(self, V, x):
+        x = np.ascontiguousarray(x, np.float64)
+        F = np.zeros_like(x)
+        ab = ctypes.c_int(0)
+        lib().qsao_residual(self._h, V, x.ctypes.data_as(ctypes.c_void_p), F.ctypes.data_as(ctypes.c_void_p),
+                            ctypes.byref(ab))
+        return F, bool(ab.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qsao_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -222,7 +222,7 @@ inline cudaError_t smem_cap(const void *kernel) {
 // every kernel launch of the library is counted (qs_kernel_launches)
 void count_launch();
 // bracket a launch with events when profiling is on: idx = prof_begin(...); launch; prof_end(h, idx)
-int prof_begin(qs_handle *h, int fam);
+int prof_begin(qs_handle *h, int fam, bool count = true);
 void prof_end(qs_handle *h, int idx);
 
 __device__ __forceinline__ double fermi_d(double w, double V, double mu, double beta) {
@@ -256,8 +256,10 @@ int sigma2_setup(qs_handle *h);
 // fp32: FFTs, 2x2 algebra and spectra in FP32 (QS_PREC_MIXED handles), Sigma written in FP64
 int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
 // autotuner (autotune.cu): kinds of decisions and the variants they choose between
-enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1, TUNE_SIG2_A = 2, TUNE_SIG2_C = 3 };
-enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2 };
+// TUNE_KELDYSH32: the Keldysh step of a mixed solve's FP32 phase, where the 3xTF32 tensor-core
+// kernel (keldysh_tf32.cu) competes with the two FP64 ones
+enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1, TUNE_SIG2_A = 2, TUNE_SIG2_C = 3, TUNE_KELDYSH32 = 4 };
+enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2, KELDYSH_TF32 = 3 };
 // the size key of a decision: the matrix order and the octave of the grid length (how many
 // energies each SM gets changes which variant wins)
 inline int tune_key(int order, int n) {

@@ -464,20 +464,21 @@ __global__ void sa_spectral(int Na, int n, const zc *__restrict__ Er, double *__
 
 int grid_for(int64_t tot, int thr = 256) { return (int)std::max<int64_t>(1, std::min<int64_t>((tot + thr - 1) / thr, 148 * 16)); }
 
-#define SA_LAUNCH(h) \
-    do {             \
-        count_launch(); \
-        QS_CUDA(&(h)->q, cudaGetLastError()); \
+// launch bracketed by the optional per-family events (qsa_profile), counted, error-checked
+#define SA_RUN(h, fam, ...)                        \
+    do {                                           \
+        const int _pi = prof_begin(&(h)->q, fam);  \
+        __VA_ARGS__;                               \
+        prof_end(&(h)->q, _pi);                    \
+        QS_CUDA(&(h)->q, cudaGetLastError());      \
     } while (0)
 
 // G_in from x: element-major sequences and G^<(t=0)
 int sa_load_input(qsa_handle *h, const double *d_x) {
     const int Na = h->Na, n = h->n;
     const int64_t tot = (int64_t)n * Na * Na;
-    sa_unpack<<<grid_for(tot), 256, 0, h->q.stream>>>(Na, n, d_x, h->d_E[0], h->d_E[1], h->d_E[2], h->d_E[3]);
-    SA_LAUNCH(h);
-    sa_glt0<<<Na, 256, 0, h->q.stream>>>(Na, n, h->d_E[2], h->delta / (2.0 * PI), h->d_Glt0);
-    SA_LAUNCH(h);
+    SA_RUN(h, K_OTHER, sa_unpack<<<grid_for(tot), 256, 0, h->q.stream>>>(Na, n, d_x, h->d_E[0], h->d_E[1], h->d_E[2], h->d_E[3]));
+    SA_RUN(h, K_OTHER, sa_glt0<<<Na, 256, 0, h->q.stream>>>(Na, n, h->d_E[2], h->delta / (2.0 * PI), h->d_Glt0));
     return 0;
 }
 
@@ -489,30 +490,24 @@ int sa_self_energies(qsa_handle *h) {
     cudaStream_t st = h->q.stream;
     zc *const *E = h->d_E;
     const dim3 gb((Nm + LT - 1) / LT, Na * Na), gs((n + LT - 1) / LT, Na * Na);
-    sa_bubbles<true><<<gb, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], pp, h->d_chi[0], h->d_chi[1], h->d_chi[2],
-                                        h->d_chi[3]);
-    SA_LAUNCH(h);
+    SA_RUN(h, K_SIG2A, sa_bubbles<true><<<gb, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], pp, h->d_chi[0], h->d_chi[1], h->d_chi[2],
+                                        h->d_chi[3]));
     if (h->order == 3) {
-        sa_bubbles<false><<<gb, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], pp, h->d_phi[0], h->d_phi[1],
-                                             h->d_phi[2], h->d_phi[3]);
-        SA_LAUNCH(h);
+        SA_RUN(h, K_SIG2A, sa_bubbles<false><<<gb, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], pp, h->d_phi[0], h->d_phi[1],
+                                             h->d_phi[2], h->d_phi[3]));
     }
     // -(i hbar)^2 and -(i hbar)^3
     const zc c2{HB * HB, 0.0}, c3{0.0, HB * HB * HB};
-    sa_sigma<<<gs, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], h->d_chi[1], h->d_chi[0], h->d_chi[2], nullptr,
-                                nullptr, nullptr, h->d_U, pp * c2, h->d_S2R, h->d_S2L);
-    SA_LAUNCH(h);
+    SA_RUN(h, K_SIG2C, sa_sigma<<<gs, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], h->d_chi[1], h->d_chi[0], h->d_chi[2], nullptr,
+                                nullptr, nullptr, h->d_U, pp * c2, h->d_S2R, h->d_S2L));
     if (h->order == 3) {
         const int64_t tot = (int64_t)Nm * Na * Na;
-        sa_products<<<grid_for(tot), 256, 0, st>>>(Na, Nm, h->d_chi[0], h->d_chi[1], h->d_chi[2], h->d_chi[3],
-                                                   h->d_U, h->d_D[0], h->d_D[1], h->d_D[2]);
-        SA_LAUNCH(h);
-        sa_products<<<grid_for(tot), 256, 0, st>>>(Na, Nm, h->d_phi[0], h->d_phi[1], h->d_phi[2], h->d_phi[3],
-                                                   h->d_U, h->d_P[0], h->d_P[1], h->d_P[2]);
-        SA_LAUNCH(h);
-        sa_sigma<<<gs, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], h->d_D[1], h->d_D[0], h->d_D[2], h->d_P[1],
-                                    h->d_P[0], h->d_P[2], h->d_U, pp * c3, h->d_S3R, h->d_S3L);
-        SA_LAUNCH(h);
+        SA_RUN(h, K_SIG2B, sa_products<<<grid_for(tot), 256, 0, st>>>(Na, Nm, h->d_chi[0], h->d_chi[1], h->d_chi[2], h->d_chi[3],
+                                                   h->d_U, h->d_D[0], h->d_D[1], h->d_D[2]));
+        SA_RUN(h, K_SIG2B, sa_products<<<grid_for(tot), 256, 0, st>>>(Na, Nm, h->d_phi[0], h->d_phi[1], h->d_phi[2], h->d_phi[3],
+                                                   h->d_U, h->d_P[0], h->d_P[1], h->d_P[2]));
+        SA_RUN(h, K_SIG2C, sa_sigma<<<gs, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], h->d_D[1], h->d_D[0], h->d_D[2], h->d_P[1],
+                                    h->d_P[0], h->d_P[2], h->d_U, pp * c3, h->d_S3R, h->d_S3L));
     }
     return 0;
 }
@@ -539,21 +534,20 @@ int sa_sweep(qsa_handle *h, double V, bool interacting, double *d_out, const dou
     cudaStream_t st = h->q.stream;
     const int ord = interacting ? h->order : 0;
     const bool s2 = interacting && h->order >= 2, s3 = interacting && h->order == 3;
-    sa_dyson_build<<<grid_for(tot), 256, 0, st>>>(Na, n, ord, h->d_H, h->d_GamL, h->d_GamR, h->d_omega,
+    SA_RUN(h, K_DYSON, sa_dyson_build<<<grid_for(tot), 256, 0, st>>>(Na, n, ord, h->d_H, h->d_GamL, h->d_GamR, h->d_omega,
                                                   s2 ? h->d_S2R : nullptr, s3 ? h->d_S3R : nullptr, h->d_U, h->d_Glt0,
-                                                  h->d_W);
-    SA_LAUNCH(h);
+                                                  h->d_W));
+    const int pi = prof_begin(&h->q, K_DYSON, false);  // the inversion counts its own launch
     int rc = invert_batched_dev(st, Na, n, h->d_W, h->d_info, h->d_ws, h->ws_slots);
+    prof_end(&h->q, pi);
     if (rc) {
         h->q.err = "batched Dyson inversion failed to launch";
         return rc;
     }
     if ((rc = sa_read_info(h))) return rc;
-    sa_keldysh_T<<<grid_for(tot), 256, 0, st>>>(Na, n, h->d_W, h->d_GamL, h->d_GamR, s2 ? h->d_S2L : nullptr,
-                                                s3 ? h->d_S3L : nullptr, h->d_omega, V, h->mu, h->beta, h->d_T);
-    SA_LAUNCH(h);
-    sa_keldysh_pack<<<grid_for(tot), 256, 0, st>>>(Na, n, h->d_W, h->d_T, d_x, d_out, h->d_gRd, h->d_gLd);
-    SA_LAUNCH(h);
+    SA_RUN(h, K_KELDYSH, sa_keldysh_T<<<grid_for(tot), 256, 0, st>>>(Na, n, h->d_W, h->d_GamL, h->d_GamR, s2 ? h->d_S2L : nullptr,
+                                                s3 ? h->d_S3L : nullptr, h->d_omega, V, h->mu, h->beta, h->d_T));
+    SA_RUN(h, K_KELDYSH, sa_keldysh_pack<<<grid_for(tot), 256, 0, st>>>(Na, n, h->d_W, h->d_T, d_x, d_out, h->d_gRd, h->d_gLd));
     // check_gf_sanity sums
     if ((rc = sum_over_energies(&h->q, h->d_gLd, Na, Na, n, h->d_sums))) return rc;
     if ((rc = sum_over_energies(&h->q, h->d_gRd, Na, Na, n, h->d_sums + Na))) return rc;
@@ -694,6 +688,13 @@ void qsa_destroy(qsa_handle *h) {
 }
 
 const char *qsa_last_error(const qsa_handle *h) { return h ? h->q.err.c_str() : "no handle"; }
+
+// per-family device time as qs_profile: dyson (W build + inversion), keldysh (products +
+// pack), sig2_fwdA slot = bubbles, sig2_mid slot = order-3 products, sig2_invC slot =
+// self-energy convolutions, broyden, reductions, other (unpack, G^<(t=0), outputs)
+int qsa_profile(qsa_handle *h, int enable, double *ms, int64_t *launches, int nfam) {
+    return qs_profile(&h->q, enable, ms, launches, nfam);
+}
 int64_t qsa_vector_length(const qsa_handle *h) { return h ? h->n_vec : -1; }
 
 // solve_scf (src/scf.f90:53-95)
@@ -740,9 +741,8 @@ int qsa_solve_scf(qsa_handle *h, double Volt, int fresh_start, qs_scf_result *re
 int qsa_current(qsa_handle *h, double Volt, double *J) {
     qs_handle *q = &h->q;
     QS_CUDA(q, cudaSetDevice(q->device));
-    sa_current<<<1, 256, 0, q->stream>>>(h->Na, h->n, h->d_E[2], h->d_E[3], h->d_GamL, h->d_omega, Volt, h->mu,
-                                         h->beta, q->d_red);
-    SA_LAUNCH(h);
+    SA_RUN(h, K_OTHER, sa_current<<<1, 256, 0, q->stream>>>(h->Na, h->n, h->d_E[2], h->d_E[3], h->d_GamL, h->d_omega, Volt, h->mu,
+                                         h->beta, q->d_red));
     double JL = 0.0;
     QS_CUDA(q, cudaMemcpyAsync(&JL, q->d_red, sizeof(double), cudaMemcpyDeviceToHost, q->stream));
     QS_CUDA(q, cudaStreamSynchronize(q->stream));
@@ -757,8 +757,7 @@ int qsa_get_observables(qsa_handle *h, double *G_less_t0, double *spectral) {
         QS_CUDA(q, cudaMemcpyAsync(G_less_t0, h->d_Glt0, sizeof(zc) * h->Na, cudaMemcpyDeviceToHost, q->stream));
     if (spectral) {
         const int64_t tot = (int64_t)h->n * h->Na;
-        sa_spectral<<<grid_for(tot), 256, 0, q->stream>>>(h->Na, h->n, h->d_E[0], h->d_spec);
-        SA_LAUNCH(h);
+        SA_RUN(h, K_OTHER, sa_spectral<<<grid_for(tot), 256, 0, q->stream>>>(h->Na, h->n, h->d_E[0], h->d_spec));
         QS_CUDA(q, cudaMemcpyAsync(spectral, h->d_spec, sizeof(double) * tot, cudaMemcpyDeviceToHost, q->stream));
     }
     QS_CUDA(q, cudaStreamSynchronize(q->stream));

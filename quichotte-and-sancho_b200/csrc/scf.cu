@@ -27,8 +27,8 @@ size_t broyden_red_len();
 static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-int prof_begin(qs_handle *h, int fam) {
-    count_launch();
+int prof_begin(qs_handle *h, int fam, bool count) {
+    if (count) count_launch();
     if (!h->prof_on) return -1;
     size_t i = h->prof_fam.size();
     if (2 * i + 2 > h->prof_ev.size()) {
@@ -284,15 +284,16 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 
 // The order-2 residual F = pack(G_out[x]) - x. QS_PREC_MIXED: while max|F| is far above the
 // FP32 noise floor, the steps form the second-order self-energies in FP32 (FFTs, 2x2
-// algebra and spectra) and the Keldysh products on the tensor cores (3xTF32,
-// keldysh_tf32.cu). The FP32 self-energies leave a noise floor of about 1e-5 in F on the
-// 120x120 helix. The solve continues in FP64 once max|F| falls below mixed_switch =
-// max(1e-5, 100 tolf), or once it has not improved for five steps while below
-// 100 mixed_switch (near the floor, where FP32 noise could stall it; far above it a stalling
-// solve gains nothing from FP64). An FP32 step whose max|F| is already below tolf is redone in
-// FP64 first, so that it cannot end the solve: convergence (max|F| < tolf) is always decided
-// on an FP64 residual, and the converged state meets the FP64 solve's criterion. The Broyden
-// pair of the first FP64 step (its dF is an FP64 residual minus an FP32 one) is not stored
+// algebra and spectra), and the Keldysh products run on the fastest of the 3xTF32
+// tensor-core kernel (keldysh_tf32.cu) and the FP64 ones (autotuned). The FP32 transforms
+// carry rounding relative to the largest spectra (|Sigma^r|, which on a fine grid is 10^3-10^4
+// times |Sigma^<|), and the Dyson inverse amplifies it by its conditioning, so the floor of F
+// depends on the model. The solve continues in FP64 once max|F| falls below mixed_switch =
+// max(1e-5, 100 tolf), or once it has not improved for five steps (a floor reached, whatever
+// its level). An FP32 step whose max|F| is already below tolf is redone in FP64 first, so
+// that it cannot end the solve: convergence (max|F| < tolf) is always decided on an FP64
+// residual, and the converged state meets the FP64 solve's criterion. The Broyden pair of
+// the first FP64 step (its dF is an FP64 residual minus an FP32 one) is not stored
 // (precision_changed).
 struct Residual2 : BroydenResidual {
     qs_handle *h;
@@ -332,7 +333,7 @@ struct Residual2 : BroydenResidual {
             since_best++;
         }
         n_mixed++;
-        if (fmax < h->mixed_switch || (since_best >= 5 && fmax < 100.0 * h->mixed_switch)) {
+        if (fmax < h->mixed_switch || since_best >= 5) {
             fp32 = false;  // the next steps are FP64
             if (fmax < h->tolf) {  // never let an FP32 residual declare convergence: redo it
                 n_mixed--;

@@ -1234,12 +1234,11 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
         k.err = h->d_info + 1;
-        // the FP32 phase of a QS_PREC_MIXED solve: G^< on the fifth-generation tensor cores
-        if (fp32 && mode == M_SCF2 && keldysh_tf32_fits(nA)) return launch_keldysh_tf32(h, k);
         const int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
         const int nbt = std::min(n, 148);
         auto launch_k = [&](int v) -> int {
             int pi;
+            if (v == KELDYSH_TF32) return launch_keldysh_tf32(h, k);
             if (v == KELDYSH_TC) {
                 QS_CUDA(h, smem_cap((const void *)keldysh_tc));
                 pi = prof_begin(h, K_KELDYSH);
@@ -1252,10 +1251,20 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
             QS_CUDA(h, cudaGetLastError());
             return 0;
         };
-        const int cand[2] = {KELDYSH_TC, KELDYSH_CUDA};
         const bool tc_ok = nA >= 32 && nA <= KD_MP && h->T_slots >= (size_t)(2 * nbt);
-        return tune_launch(h, TUNE_KELDYSH, tune_key(nA, n), tc_ok ? cand : cand + 1, tc_ok ? 2 : 1,
-                           (tc_ok && nA >= 48) ? KELDYSH_TC : KELDYSH_CUDA, launch_k);
+        const int fallback = (tc_ok && nA >= 48) ? KELDYSH_TC : KELDYSH_CUDA;
+        // the FP32 phase of a QS_PREC_MIXED solve: the 3xTF32 kernel on the fifth-generation
+        // tensor cores is a candidate too, kept only where it is the fastest
+        if (fp32 && mode == M_SCF2 && keldysh_tf32_fits(nA)) {
+            int c3[3], nc = 0;
+            c3[nc++] = KELDYSH_TF32;
+            if (tc_ok) c3[nc++] = KELDYSH_TC;
+            c3[nc++] = KELDYSH_CUDA;
+            return tune_launch(h, TUNE_KELDYSH32, tune_key(nA, n), c3, nc, fallback, launch_k);
+        }
+        const int cand[2] = {KELDYSH_TC, KELDYSH_CUDA};
+        return tune_launch(h, TUNE_KELDYSH, tune_key(nA, n), tc_ok ? cand : cand + 1, tc_ok ? 2 : 1, fallback,
+                           launch_k);
     }
     // chunked full inversion + per-energy outputs
     const int Mrows = (mode == M_FINAL) ? N : nA;

@@ -162,7 +162,7 @@ C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current
          "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
          "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice",
          "qs_hermitian_eigensystem", "qs_hermitian_eigenvalues", "qs_dftb_lowdin")
-TUNE_DYSON, TUNE_KELDYSH, TUNE_SIG2_A, TUNE_SIG2_C = 0, 1, 2, 3
+TUNE_DYSON, TUNE_KELDYSH, TUNE_SIG2_A, TUNE_SIG2_C, TUNE_KELDYSH32 = 0, 1, 2, 3, 4
 QS_ERR_NOALLOC_LIMIT = -1001
 QS_ERR_TOO_LARGE = -1002
 

@@ -33,7 +33,8 @@ _ptr = qb._ptr
 
 # every entry point of include/qsa200.h
 C_ABI = ("qsa_create", "qsa_destroy", "qsa_last_error", "qsa_vector_length", "qsa_solve_scf", "qsa_current",
-         "qsa_get_observables", "qsa_initial_vector", "qsa_residual", "qsa_self_energies")
+         "qsa_get_observables", "qsa_initial_vector", "qsa_residual", "qsa_self_energies", "qsa_profile")
+KERNEL_FAMILIES = ("dyson", "keldysh", "bubbles", "products", "sigma", "unused", "broyden", "reductions", "other")
 
 
 class _QsahModel(ctypes.Structure):
@@ -75,6 +76,8 @@ def bind_solver(lib, prefix):
     f("residual").argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                               ctypes.POINTER(ctypes.c_int)]
     f("self_energies").argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
+    if hasattr(lib, prefix + "profile"):
+        f("profile").argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
     return lib
 
 
@@ -199,6 +202,14 @@ class SanchoSolver:
         ab = ctypes.c_int(0)
         self._check(self._f("residual")(self._h, V, _ptr(x), _ptr(F), ctypes.byref(ab)), "residual")
         return F, bool(ab.value)
+
+    def profile(self, enable):
+        """Per-family device time (ms) and launch counts since the last call (qsa_profile)."""
+        ms = np.zeros(len(KERNEL_FAMILIES))
+        cnt = np.zeros(len(KERNEL_FAMILIES), np.int64)
+        flag = -1 if enable is None else int(bool(enable))
+        self._f("profile")(self._h, flag, _ptr(ms), _ptr(cnt), len(KERNEL_FAMILIES))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_FAMILIES)}
 
     def self_energies(self, x):
         """Sigma2^r, Sigma2^<, Sigma3^r, Sigma3^< as (N_sites, N_sites, n_omega) arrays."""

@@ -30,7 +30,7 @@ def test_cuda_library_exports_every_sancho_entry_point():
     import sancho_b200 as sb
     lib = ctypes.CDLL(qb.LIB_PATH)
     names = [n for n in declared("qsa200.h") if n.startswith("qsa_")]
-    assert len(names) == 10
+    assert len(names) == 11
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(sb.C_ABI) == set(names)
