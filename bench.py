@@ -273,12 +273,12 @@ def make_cfg2_case(path, n_omega=32768, seed=40):
         for a, _ in orb:
             f.write(f"{0.8 if a in inter else 0.0}\n")
 
-    def write_input(dw, up, delta):
+    def write_input(dw, up, delta, mu=0.0):
         with open(os.path.join(path, "input.dat"), "w") as f:
             f.write("hamiltonian = dftb_hs\nham_file = hamsqr1.dat\noverlap_file = oversqr.dat\n"
                     "xyz_file = molecule.xyz\nmax_angular_momentum = C:p H:s\nsoc_xi = C:0.00849\n"
                     "soc_form = dual\nlead_left_atoms = 1\nlead_right_atoms = 28\nhubbard_file = U_per_orbital.dat\n"
-                    f"T = 300.d0\nV = 0.1d0\nVf = 0.3d0\ndelv = 0.1d0\nmu = 0.0d0\norder = 2\nU_int = 0.8d0\n"
+                    f"T = 300.d0\nV = 0.1d0\nVf = 0.3d0\ndelv = 0.1d0\nmu = {float(mu)!r}\norder = 2\nU_int = 0.8d0\n"
                     f"GammaL_up = 0.5d0\nGammaL_down = 0.5d0\nGammaR = 0.5d0\ndw = {float(dw)!r}\n"
                     f"up = {float(up)!r}\ndelta = {float(delta)!r}\n")
     write_input(1.0, 1.0, 0.05)
@@ -286,11 +286,15 @@ def make_cfg2_case(path, n_omega=32768, seed=40):
 
 
 def model_cfg2(qb, path, n_omega):
-    """The cfg2 case loaded through the host layer, its grid fitted to n_omega points."""
+    """The cfg2 case loaded through the host layer, its grid fitted to n_omega points, with mu
+    in the middle of the widest gap between the spin-orbital levels within 20 of half filling
+    (the synthetic molecule's spectrum is dense there: 30-180 meV spacings)."""
     write_input = make_cfg2_case(path, n_omega)
-    ev = qb.Model.load(path).Ev
+    ev = np.sort(qb.Model.load(path).Ev)
     delta = (ev[-1] - ev[0] + 2.0) / n_omega
-    write_input(1.0, 1.0 + 0.5 * delta, delta)
+    half = len(ev) // 2
+    k = half - 20 + int(np.argmax(np.diff(ev[half - 20:half + 21])))
+    write_input(1.0, 1.0 + 0.5 * delta, delta, mu=0.5 * (ev[k] + ev[k + 1]))
     m = qb.Model.load(path)
     assert m.n_omega == n_omega, m.n_omega
     return m
@@ -564,8 +568,8 @@ def run_case(args, device):
     return 0
 
 
-SANCHO_CHAIN = dict(N_sites=10, E_CC=2.0, t_hop=-0.4, U_int=0.8, GammaL=1.0, GammaR=1.0, T=300.0, mu=2.0, dw=1.0,
-                    up=1.0, delta=0.002, order=3)
+SANCHO_CHAIN = dict(N_sites=10, E_CC=2.0, t_hop=-0.4, U_int=0.5, GammaL=1.0, GammaR=1.0, T=300.0, mu=2.0, dw=1.0,
+                    up=1.0, delta=0.004, order=3)
 SANCHO_VOLTS = [-0.5, -0.25, 0.0, 0.25, 0.5]
 
 
@@ -582,8 +586,8 @@ def sancho_input(path, chain, volts):
 
 
 def run_sancho(args, device):
-    """--case sancho: SANCHO's order-3 chain (10 sites, 1740 energies; SANCHO's regression case
-    scaled up: the same chain and settings, a finer grid and more sites) swept over five
+    """--case sancho: SANCHO's order-3 chain (10 sites, 883 energies, U 0.5 eV; SANCHO's
+    regression case scaled up: the same chain, a finer grid and more sites) swept over five
     voltages with continuation on the B200 solver (include/qsa200.h), its kernel families
     against the FP64 roofline, and the CPU oracle's time per SCF iteration of the same sweep."""
     import tempfile
@@ -636,7 +640,7 @@ def run_sancho(args, device):
     line = {"metric": "converged IV points/s", "value": conv / wall if wall > 0 else 0.0, "unit": "IV points/s",
             "n_gpus": 1, "steps": len(SANCHO_VOLTS), "warmup": 1, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic", "case": "sancho",
-            "config": {"workload": f"SANCHO chain, {Na} sites, order 3, {n} energies (delta 0.002 eV), U 0.8 eV, "
+            "config": {"workload": f"SANCHO chain, {Na} sites, order 3, {n} energies (delta 0.004 eV), U 0.5 eV, "
                                    "E_CC 2 eV, t -0.4 eV, Gamma 1 eV, T 300 K, mu 2 eV; V -0.5..0.5 step 0.25 with "
                                    "continuation; alpha_mix 0.3, nhist 8, tolf 1e-6 (SANCHO's defaults)"},
             "scf_iterations": [p["n_iter"] for p in pts], "converged": [p["converged"] for p in pts],
@@ -927,6 +931,7 @@ def main():
             "converged": [bool(p["converged"]) for p in pts],
             "scf_steps_per_point": [p["n_iter"] for p in pts],
             "converged_points": n_conv,
+            "fp32_steps_per_point": [p["n_mixed"] for p in pts] if prec_name == "mixed" else None,
             "e2e": {"value": n_conv / wall if wall > 0 else 0.0, "unit": "IV points/s", "h2d_bytes_per_step": 8,
                     "d2h_bytes_per_step": obs_bytes},
             "gpu_launches": launches,

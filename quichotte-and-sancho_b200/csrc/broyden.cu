@@ -361,7 +361,13 @@ int broyden_solve_dev(qs_handle *h, BroydenResidual &res, double *&d_x, double *
             out.converged = true;
             break;
         }
-        // history pair, Gram column, dF^T F
+        // history pair, Gram column, dF^T F. A residual that changed precision (the FP32
+        // phase of a mixed solve ending) starts a new history: the stored pairs model the
+        // other residual function
+        if (res.precision_changed()) {
+            nstored = 0;
+            nh = 0;
+        }
         bool store = want_dn && fnorm > 0.0 && !res.precision_changed();
         int slot = want_dn ? nstored % nhist : 0;
         int nh_new = store ? std::min(nstored + 1, nhist) : std::min(nstored, nhist);

@@ -3,7 +3,7 @@
 // SL = i (f_L Gamma_L + f_R Gamma_R) + Sigma2^<, written into the SCF residual as
 // F = pack(G_out) - x (src/scf.f90:158-188; pack_gf common/linear_algebra.f90:155-191).
 //
-// One CTA of 4 warps per SM walks the energies. Both complex products (T = G SL, then
+// One CTA of 16 warps per SM walks the energies. Both complex products (T = G SL, then
 // L = T G^dagger) run as tcgen05.mma of kind tf32 with FP32 accumulators in tensor memory:
 // each operand x is split into two TF32 parts x = hi + lo (round to nearest), and each real
 // product a b is formed as a_hi b_hi + a_hi b_lo + a_lo b_hi ("3xTF32"), which keeps close
@@ -13,11 +13,16 @@
 //     tensor core's K-major core-matrix layout (tcgen05.cuh), double-buffered: the chunk
 //     after the next is staged while the tensor core works on the current one, and a
 //     buffer is refilled only once the mbarrier signalled by tcgen05.commit says the MMAs
-//     that read it completed.
+//     that read it completed. Every thread stages one (row, k-quad) of each operand: the
+//     G^r columns are read with consecutive rows on consecutive lanes, the SL rows (Sigma2^<
+//     is column-major, SL(k, n) at k + n nA) with four consecutive k per lane, so that all
+//     loads are coalesced, and 16 warps keep enough of them in flight to cover the latency
+//     of the global reads (the conversion and split run on the CUDA cores).
 //   * TMEM holds T (columns 0-255: real, imaginary) and L (256-511). The second product reads
 //     T back from TMEM (tcgen05.ld), splits it and stages it as its A operand.
-//   * The epilogue reads L from TMEM (lane = row), writes the upper triangle of G^< minus x
-//     into F, the diagonal into gLd, and copies G^r - x (FP64) into the G^r part of F.
+//   * The epilogue reads L from TMEM (lane = row; the four warps of a lane quarter take
+//     different 32-column blocks), writes the upper triangle of G^< minus x into F, the
+//     diagonal into gLd, and copies G^r - x (FP64) into the G^r part of F.
 // The G^r part of F is exact (FP64 from the Dyson kernel); the G^< part carries the
 // rounding of the FP32 products (relative ~1e-7), which the FP32 phase tolerates (the
 // residual switches to the FP64 kernels before max|F| approaches that level).
@@ -41,7 +46,7 @@ constexpr int KT_NCH = KT_M / KT_KC;       // chunks per product
 constexpr int KT_TILE = KT_M * KT_KC * 4;  // one 128 x 16 TF32 tile: 8 KB
 constexpr int KT_BUF = 8 * KT_TILE;        // A (re hi, re lo, im hi, im lo) + B (the same)
 constexpr int KT_SMEM = 2 * KT_BUF;        // two buffers: 128 KB
-constexpr int KT_THREADS = 128;
+constexpr int KT_THREADS = 512;  // 16 warps: 4 lane quarters x 4
 constexpr uint32_t KT_TMEM_COLS = 512;     // T re, T im, L re, L im: 128 columns each
 
 // one 4-element k-quad of row r (real and imaginary parts) split into the 4 tiles of a half
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(KT_THREADS, 1) keldysh_tf32(KeldyshArgs a) {
     fence_after_sync();
     const uint32_t tm = tslot, tT = tm, tL = tm + 2 * KT_M;
     const uint32_t sbase = smem_u32(sm);
-    const uint32_t lanes = (uint32_t)(32 * warp) << 16;  // this warp's TMEM lane quarter
+    const uint32_t lanes = (uint32_t)(32 * (warp & 3)) << 16;  // this warp's TMEM lane quarter
     const int64_t offL = 2 * (int64_t)nfull, offD = offL + (int64_t)nA * (nA - 1);
     int g = 0;  // chunks staged so far: buffer g & 1, mbarrier phase g >> 1
     bool ok = true;
@@ -120,33 +125,40 @@ __global__ void __launch_bounds__(KT_THREADS, 1) keldysh_tf32(KeldyshArgs a) {
         const double w = a.omega[iw];
         const double fL = fermi_d(w, a.V, a.mu, a.beta), fR = fermi_d(w, 0.0, a.mu, a.beta);
         const zc *SL2 = a.SigL ? a.SigL + (size_t)iw * nfull : nullptr;
-        // ---- T = G SL: A row m = tid (G(m, k)), B row n = tid (SL(k, n))
+        // ---- T = G SL: thread (m = tid % 128, quad tid / 128) stages A = G(m, k), thread
+        // (n = tid / 4, quad tid % 4) stages B = SL(k, n)
         for (int c = 0; c < KT_NCH; c++, g++) {
             if (!(ok = wait_chunk(g - 2))) break;
             unsigned char *buf = sm + (g & 1) * KT_BUF;
-            const int r = tid;
-#pragma unroll
-            for (int q = 0; q < KT_NQ; q++) {
-                float are[4], aim[4], bre[4], bim[4];
+            {
+                const int m = tid & (KT_M - 1), q = tid >> 7;
+                float re[4], im[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int k = KT_KC * c + 4 * q + e;
-                    const bool v = r < nA && k < nA;
-                    const zc gv = v ? G[r + (size_t)k * nA] : zc{0, 0};
+                    const zc gv = (m < nA && k < nA) ? G[m + (size_t)k * nA] : zc{0, 0};
+                    re[e] = (float)gv.x;
+                    im[e] = (float)gv.y;
+                }
+                put_quad(buf, m, q, re, im);
+            }
+            {
+                const int n = tid >> 2, q = tid & 3;
+                float re[4], im[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int k = KT_KC * c + 4 * q + e;
                     zc s{0, 0};
-                    if (v) {  // SL(k, r) = i (fL GamL_s + fR GamR_s) / hbar + Sigma2^<  (src/scf.f90:333-336)
-                        const size_t idx = k + (size_t)r * nA;
+                    if (n < nA && k < nA) {  // SL(k, n) = i (fL GamL_s + fR GamR_s) / hbar + Sigma2^<  (src/scf.f90:333-336)
+                        const size_t idx = k + (size_t)n * nA;
                         const zc gl = a.GamLs[idx], gr = a.GamRs[idx];
                         const zc s2 = SL2 ? SL2[idx] : zc{0, 0};
                         s = zc{-(fL * gl.y + fR * gr.y) + s2.x, fL * gl.x + fR * gr.x + s2.y};
                     }
-                    are[e] = (float)gv.x;
-                    aim[e] = (float)gv.y;
-                    bre[e] = (float)s.x;
-                    bim[e] = (float)s.y;
+                    re[e] = (float)s.x;
+                    im[e] = (float)s.y;
                 }
-                put_quad(buf, r, q, are, aim);
-                put_quad(buf + 4 * KT_TILE, r, q, bre, bim);
+                put_quad(buf + 4 * KT_TILE, n, q, re, im);
             }
             fence_async_smem();
             __syncthreads();
@@ -158,11 +170,12 @@ __global__ void __launch_bounds__(KT_THREADS, 1) keldysh_tf32(KeldyshArgs a) {
         }
         if (!ok || !(ok = wait_chunk(g - 1))) break;  // T complete
         fence_after_sync();
-        // ---- L = T G^dagger: A row = TMEM lane (T from tensor memory), B row n = tid
+        // ---- L = T G^dagger: warps 0-3 stage A = T from tensor memory (row = TMEM lane),
+        // thread (n = tid % 128, quad tid / 128) stages B(k, n) = conj G(n, k)
         for (int c = 0; c < KT_NCH; c++, g++) {
             if (!(ok = wait_chunk(g - 2))) break;
             unsigned char *buf = sm + (g & 1) * KT_BUF;
-            {
+            if (warp < 4) {
                 float tr[16], ti[16];
                 tmem_ld16(tT + lanes + KT_KC * c, tr);
                 tmem_ld16(tT + lanes + KT_M + KT_KC * c, ti);
@@ -174,9 +187,8 @@ __global__ void __launch_bounds__(KT_THREADS, 1) keldysh_tf32(KeldyshArgs a) {
                     put_quad(buf, r, q, re, im);
                 }
             }
-            const int n = tid;
-#pragma unroll
-            for (int q = 0; q < KT_NQ; q++) {
+            {
+                const int n = tid & (KT_M - 1), q = tid >> 7;
                 float bre[4], bim[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
@@ -200,8 +212,8 @@ __global__ void __launch_bounds__(KT_THREADS, 1) keldysh_tf32(KeldyshArgs a) {
         // ---- epilogue: the upper triangle of G^< and its diagonal, then G^r, minus x
         double *blk = a.out + (size_t)iw * a.nblk;
         const double *xb = a.xsub ? a.xsub + (size_t)iw * a.nblk : nullptr;
-        const int r = 32 * warp + lane;
-        for (int j = 0; 32 * j < nA; j++) {  // warp-uniform
+        const int r = 32 * (warp & 3) + lane;
+        for (int j = warp >> 2; 32 * j < nA; j += KT_THREADS / 128) {  // warp-uniform
             float lr[32], li[32];
             tmem_ld32(tL + lanes + 32 * j, lr);
             tmem_ld32(tL + lanes + KT_M + 32 * j, li);

@@ -305,7 +305,8 @@ void release_all(qs_handle *h);
 struct BroydenResidual {
     virtual int operator()(const double *d_x, double *d_F, bool &abort) = 0;
     // true if the residual just evaluated used another precision than the one before: the
-    // (dF, u) pair of this step would mix two different residual functions and is not stored
+    // (dF, u) pair of this step would mix two different residual functions and is not
+    // stored, and the history built on the other function is dropped
     virtual bool precision_changed() const { return false; }
     virtual ~BroydenResidual() = default;
 };

@@ -87,8 +87,10 @@ struct qsa_handle {
 
 namespace {
 
-constexpr int LT = 128;          // outputs per block and summation values per tile
-constexpr int LW = 2 * LT - 1;   // B window of a tile
+constexpr int LT = 128;          // threads per block and summation values per tile
+constexpr int NP = 2 * LT;       // outputs per block: two adjacent ones per thread
+constexpr int LW = LT + NP - 1;  // B window of a tile
+constexpr int LH = (LW + 1) / 2; // the window is stored de-interleaved: even slots, then odd ones
 constexpr double HB = 1.0;       // hbar (common/constants.f90:19)
 
 // ---------------------------------------------------------------------------------
@@ -147,20 +149,27 @@ __global__ void sa_glt0(int Na, int n, const zc *__restrict__ EL, double pp, zc 
 // ---------------------------------------------------------------------------------
 // Lag sums. Output p of an element, summation index j in [0, n): the B index is
 // b = SG*j + TG*p + c. A tile covers j in [J0, J0 + LT) and the block's outputs
-// p in [P0, P0 + LT), so it touches b in a window of LW values.
+// p in [P0, P0 + NP), so it touches b in a window of LW values (slot = b - wbase).
+// Thread t owns the adjacent outputs 2t and 2t + 1: at a given j the second needs the
+// window value TG slots from the first's, which is the value the first needed one step
+// earlier in the walk (j ascending for (SG, TG) = (+1, -1) and (-1, +1), descending for
+// (+1, +1)); so each step loads one window value per B sequence for two outputs. The
+// window is stored with its even slots first and its odd slots after them: the lanes of a
+// warp read slots 2t + const, which land on consecutive 16-byte words.
 // ---------------------------------------------------------------------------------
 template <int SG, int TG>
 struct LagMap {
+    static constexpr bool ASC = !(SG > 0 && TG > 0);  // the order of the walk over a tile
     __device__ static int wbase(int J0, int P0, int c) {
-        return SG * (SG > 0 ? J0 : J0 + LT - 1) + TG * (TG > 0 ? P0 : P0 + LT - 1) + c;
+        return SG * (SG > 0 ? J0 : J0 + LT - 1) + TG * (TG > 0 ? P0 : P0 + NP - 1) + c;
     }
-    // window slot of (J0 + jj, P0 + tp)
+    // window slot of (J0 + jj, P0 + tp), in [0, LW)
     __device__ static int slot(int jj, int tp) {
-        return SG * (SG > 0 ? jj : jj - (LT - 1)) + TG * (TG > 0 ? tp : tp - (LT - 1));
+        return SG * (SG > 0 ? jj : jj - (LT - 1)) + TG * (TG > 0 ? tp : tp - (NP - 1));
     }
     // j range (inclusive) with b in [0, Lb) for some p of the block, within [0, n)
     __device__ static void jrange(int P0, int c, int Lb, int n, int &jlo, int &jhi) {
-        const int t0 = TG * P0, t1 = TG * (P0 + LT - 1);
+        const int t0 = TG * P0, t1 = TG * (P0 + NP - 1);
         const int tmin = min(t0, t1), tmax = max(t0, t1);
         if (SG > 0) {
             jlo = -tmax - c;
@@ -173,11 +182,12 @@ struct LagMap {
         jhi = min(jhi, n - 1);
     }
 };
+__device__ __forceinline__ int wpos(int u) { return (u & 1) * LH + (u >> 1); }
 
 // stage NA sequences of A at [J0, J0 + LT) and NB sequences of B on the tile's window
 template <int NA, int NB>
 __device__ __forceinline__ void lag_stage(const zc *const (&A)[NA], const zc *const (&B)[NB], int n, int Lb, int J0,
-                                          int wb, zc (*sA)[LT], zc (*sB)[2 * LT]) {
+                                          int wb, zc (*sA)[LT], zc (*sB)[2 * LH]) {
     const int t = threadIdx.x;
 #pragma unroll
     for (int s = 0; s < NA; s++) {
@@ -188,11 +198,46 @@ __device__ __forceinline__ void lag_stage(const zc *const (&A)[NA], const zc *co
     for (int s = 0; s < NB; s++)
         for (int u = t; u < LW; u += LT) {
             const int b = wb + u;
-            sB[s][u] = (b >= 0 && b < Lb) ? B[s][b] : zc{0.0, 0.0};
+            sB[s][wpos(u)] = (b >= 0 && b < Lb) ? B[s][b] : zc{0.0, 0.0};
         }
 }
 
-// compute_bubbles (src/self_energies.f90:49-115). Grid (ceil(Nm/LT), Na^2), block LT.
+// The tiles of one lag sum for the thread's outputs 2t, 2t + 1: step(a, cur, prev) gets
+// the NA values of A at j, the NB window values of output 2t (cur) and of output 2t + 1
+// (prev, the previous step's cur).
+template <int SG, int TG, int NA, int NB, class Step>
+__device__ __forceinline__ void lag_walk(const zc *const (&A)[NA], const zc *const (&B)[NB], int n, int Lb, int P0,
+                                         int c, zc (*sA)[LT], zc (*sB)[2 * LH], Step step) {
+    using M = LagMap<SG, TG>;
+    int jlo, jhi;
+    M::jrange(P0, c, Lb, n, jlo, jhi);
+    const int tp = 2 * threadIdx.x;
+    for (int J0 = jlo; J0 <= jhi; J0 += LT) {
+        __syncthreads();
+        lag_stage<NA, NB>(A, B, n, Lb, J0, M::wbase(J0, P0, c), sA, sB);
+        __syncthreads();
+        const int nj = min(LT, jhi - J0 + 1);
+        zc prev[NB], cur[NB], av[NA];
+        {
+            const int w1 = wpos(M::slot(M::ASC ? 0 : nj - 1, tp) + TG);
+#pragma unroll
+            for (int s = 0; s < NB; s++) prev[s] = sB[s][w1];
+        }
+        for (int it = 0; it < nj; it++) {
+            const int jj = M::ASC ? it : nj - 1 - it;
+            const int w0 = wpos(M::slot(jj, tp));
+#pragma unroll
+            for (int s = 0; s < NB; s++) cur[s] = sB[s][w0];
+#pragma unroll
+            for (int s = 0; s < NA; s++) av[s] = sA[s][jj];
+            step(av, cur, prev);
+#pragma unroll
+            for (int s = 0; s < NB; s++) prev[s] = cur[s];
+        }
+    }
+}
+
+// compute_bubbles (src/self_energies.f90:49-115). Grid (ceil(Nm/NP), Na^2), block LT.
 //   PH (chi, m = p - (n-1)): A = {G^>, G^<, G^r, G^a}_ab (k1), B = {G^<, G^>, G^a, G^r}_ba (k1 - m)
 //   PP (phi, q0 = p):        A = {G^>, G^<, G^r, G^a}_ab (k1), B = {G^>, G^<, G^r, G^a}_ab (q0 - k1)
 // with the same products: s1 = A0 B0, s2 = A1 B1, s3 = A2 B0 + A1 B2, s4 = A3 B0 + A1 B3
@@ -203,9 +248,7 @@ __global__ void __launch_bounds__(LT) sa_bubbles(int Na, int n, const zc *__rest
                                                  zc *__restrict__ oG, zc *__restrict__ oL, zc *__restrict__ oR,
                                                  zc *__restrict__ oA) {
     __shared__ zc sA[4][LT];
-    __shared__ zc sB[4][2 * LT];
-    constexpr int SGN = PH ? 1 : -1, TGN = PH ? -1 : 1;
-    using M = LagMap<SGN, TGN>;
+    __shared__ zc sB[4][2 * LH];
     const int Nm = 2 * n - 1, e = blockIdx.y, a = e % Na, b = e / Na;
     const int eb = PH ? (b + a * Na) : e;
     const size_t oe = (size_t)e * n, ob = (size_t)eb * n;
@@ -213,38 +256,37 @@ __global__ void __launch_bounds__(LT) sa_bubbles(int Na, int n, const zc *__rest
     const zc *const B[4] = {PH ? EL + ob : EG + ob, PH ? EG + ob : EL + ob, PH ? Ea + ob : Er + ob,
                             PH ? Er + ob : Ea + ob};
     const int c = PH ? (n - 1) : 0;  // chi: b = k1 - (p - (n-1)); phi: b = p - k1
-    const int P0 = blockIdx.x * LT, p = P0 + threadIdx.x;
-    int jlo, jhi;
-    M::jrange(P0, c, n, n, jlo, jhi);
-    zc s1{0, 0}, s2{0, 0}, s3{0, 0}, s4{0, 0};
-    for (int J0 = jlo; J0 <= jhi; J0 += LT) {
-        __syncthreads();
-        lag_stage<4, 4>(A, B, n, n, J0, M::wbase(J0, P0, c), sA, sB);
-        __syncthreads();
-        const int nj = min(LT, jhi - J0 + 1);
-        for (int jj = 0; jj < nj; jj++) {
-            const int w = M::slot(jj, threadIdx.x);
-            const zc a0 = sA[0][jj], a1 = sA[1][jj], a2 = sA[2][jj], a3 = sA[3][jj];
-            const zc b0 = sB[0][w], b1 = sB[1][w], b2 = sB[2][w], b3 = sB[3][w];
-            cfma(s1, a0, b0);
-            cfma(s2, a1, b1);
-            cfma(s3, a2, b0);
-            cfma(s3, a1, b2);
-            cfma(s4, a3, b0);
-            cfma(s4, a1, b3);
+    const int P0 = blockIdx.x * NP, p = P0 + 2 * threadIdx.x;
+    zc s[2][4] = {};
+    auto step = [&](const zc (&av)[4], const zc (&b0)[4], const zc (&b1)[4]) {
+        cfma(s[0][0], av[0], b0[0]);
+        cfma(s[0][1], av[1], b0[1]);
+        cfma(s[0][2], av[2], b0[0]);
+        cfma(s[0][2], av[1], b0[2]);
+        cfma(s[0][3], av[3], b0[0]);
+        cfma(s[0][3], av[1], b0[3]);
+        cfma(s[1][0], av[0], b1[0]);
+        cfma(s[1][1], av[1], b1[1]);
+        cfma(s[1][2], av[2], b1[0]);
+        cfma(s[1][2], av[1], b1[2]);
+        cfma(s[1][3], av[3], b1[0]);
+        cfma(s[1][3], av[1], b1[3]);
+    };
+    if (PH) lag_walk<1, -1, 4, 4>(A, B, n, n, P0, c, sA, sB, step);
+    else lag_walk<-1, 1, 4, 4>(A, B, n, n, P0, c, sA, sB, step);
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+        if (p + r < Nm) {
+            const size_t o = (size_t)e * Nm + p + r;
+            oG[o] = pp * s[r][0];
+            oL[o] = pp * s[r][1];
+            oR[o] = pp * s[r][2];
+            oA[o] = pp * s[r][3];
         }
-    }
-    if (p < Nm) {
-        const size_t o = (size_t)e * Nm + p;
-        oG[o] = pp * s1;
-        oL[o] = pp * s2;
-        oR[o] = pp * s3;
-        oA[o] = pp * s4;
-    }
 }
 
 // second_order_sigma / third_order_sigma step 3 (src/self_energies.f90:117-207).
-// Grid (ceil(n/LT), Na^2), block LT; p = iw, j = kk.
+// Grid (ceil(n/NP), Na^2), block LT; p = iw, j = kk.
 //   particle-hole part: A = {G^<, G^>, G^r}_ij (kk), B = {X^<, X^>, X^r}_ij (m = iw - kk)
 //   particle-particle part (order 3): A = {G^>, G^<, G^a}_ji (kk), B = {P^<, P^>, P^r}_ij (iw + kk)
 // a^< += A0 B0, a^r += A2 B1 + A0 B2; Sigma = f a with f = c U_i U_j delta/2pi.
@@ -256,59 +298,40 @@ __global__ void __launch_bounds__(LT) sa_sigma(int Na, int n, const zc *__restri
                                                const double *__restrict__ U, zc fc, zc *__restrict__ SR,
                                                zc *__restrict__ SL) {
     __shared__ zc sA[3][LT];
-    __shared__ zc sB[3][2 * LT];
+    __shared__ zc sB[3][2 * LH];
     const int Nm = 2 * n - 1, e = blockIdx.y, i = e % Na, j = e / Na;
-    const int P0 = blockIdx.x * LT, p = P0 + threadIdx.x;
-    zc aL{0, 0}, aR{0, 0};
+    const int P0 = blockIdx.x * NP, p = P0 + 2 * threadIdx.x;
+    zc aL[2] = {}, aR[2] = {};
+    auto step = [&](const zc (&av)[3], const zc (&b0)[3], const zc (&b1)[3]) {
+        cfma(aL[0], av[0], b0[0]);
+        cfma(aR[0], av[2], b0[1]);
+        cfma(aR[0], av[0], b0[2]);
+        cfma(aL[1], av[0], b1[0]);
+        cfma(aR[1], av[2], b1[1]);
+        cfma(aR[1], av[0], b1[2]);
+    };
     {
-        using M = LagMap<-1, 1>;  // chi index m + n - 1 = iw - kk + n - 1
-        const int c = n - 1;
+        // chi index m + n - 1 = iw - kk + n - 1
         const size_t oe = (size_t)e * n, ox = (size_t)e * Nm;
         const zc *const A[3] = {EL + oe, EG + oe, Er + oe};
         const zc *const B[3] = {XL + ox, XG + ox, XR + ox};
-        int jlo, jhi;
-        M::jrange(P0, c, Nm, n, jlo, jhi);
-        for (int J0 = jlo; J0 <= jhi; J0 += LT) {
-            __syncthreads();
-            lag_stage<3, 3>(A, B, n, Nm, J0, M::wbase(J0, P0, c), sA, sB);
-            __syncthreads();
-            const int nj = min(LT, jhi - J0 + 1);
-            for (int jj = 0; jj < nj; jj++) {
-                const int w = M::slot(jj, threadIdx.x);
-                const zc a0 = sA[0][jj], a2 = sA[2][jj];
-                cfma(aL, a0, sB[0][w]);
-                cfma(aR, a2, sB[1][w]);
-                cfma(aR, a0, sB[2][w]);
-            }
-        }
+        lag_walk<-1, 1, 3, 3>(A, B, n, Nm, P0, n - 1, sA, sB, step);
     }
     if (PL) {
-        using M = LagMap<1, 1>;  // q0 = iw + kk
+        // q0 = iw + kk
         const size_t oe = ((size_t)j + (size_t)i * Na) * n, ox = (size_t)e * Nm;
         const zc *const A[3] = {EG + oe, EL + oe, Ea + oe};
         const zc *const B[3] = {PL + ox, PG + ox, PR + ox};
-        int jlo, jhi;
-        M::jrange(P0, 0, Nm, n, jlo, jhi);
-        for (int J0 = jlo; J0 <= jhi; J0 += LT) {
-            __syncthreads();
-            lag_stage<3, 3>(A, B, n, Nm, J0, M::wbase(J0, P0, 0), sA, sB);
-            __syncthreads();
-            const int nj = min(LT, jhi - J0 + 1);
-            for (int jj = 0; jj < nj; jj++) {
-                const int w = M::slot(jj, threadIdx.x);
-                const zc a0 = sA[0][jj], a2 = sA[2][jj];
-                cfma(aL, a0, sB[0][w]);
-                cfma(aR, a2, sB[1][w]);
-                cfma(aR, a0, sB[2][w]);
-            }
+        lag_walk<1, 1, 3, 3>(A, B, n, Nm, P0, 0, sA, sB, step);
+    }
+    const zc f = (U[i] * U[j]) * fc;
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+        if (p + r < n) {
+            const size_t o = (size_t)e + (size_t)(p + r) * Na * Na;
+            SR[o] = f * aR[r];
+            SL[o] = f * aL[r];
         }
-    }
-    if (p < n) {
-        const zc f = (U[i] * U[j]) * fc;
-        const size_t o = (size_t)e + (size_t)p * Na * Na;
-        SR[o] = f * aR;
-        SL[o] = f * aL;
-    }
 }
 
 // third_order_sigma step 2 (src/self_energies.f90:160-185): per m (or q0) and (i, j)
@@ -489,7 +512,7 @@ int sa_self_energies(qsa_handle *h) {
     const double pp = h->delta / (2.0 * PI);
     cudaStream_t st = h->q.stream;
     zc *const *E = h->d_E;
-    const dim3 gb((Nm + LT - 1) / LT, Na * Na), gs((n + LT - 1) / LT, Na * Na);
+    const dim3 gb((Nm + NP - 1) / NP, Na * Na), gs((n + NP - 1) / NP, Na * Na);
     SA_RUN(h, K_SIG2A, sa_bubbles<true><<<gb, LT, 0, st>>>(Na, n, E[0], E[1], E[2], E[3], pp, h->d_chi[0], h->d_chi[1], h->d_chi[2],
                                         h->d_chi[3]));
     if (h->order == 3) {

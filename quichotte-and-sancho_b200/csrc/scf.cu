@@ -289,12 +289,12 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 // carry rounding relative to the largest spectra (|Sigma^r|, which on a fine grid is 10^3-10^4
 // times |Sigma^<|), and the Dyson inverse amplifies it by its conditioning, so the floor of F
 // depends on the model. The solve continues in FP64 once max|F| falls below mixed_switch =
-// max(1e-5, 100 tolf), or once it has not improved for five steps (a floor reached, whatever
-// its level). An FP32 step whose max|F| is already below tolf is redone in FP64 first, so
-// that it cannot end the solve: convergence (max|F| < tolf) is always decided on an FP64
-// residual, and the converged state meets the FP64 solve's criterion. The Broyden pair of
-// the first FP64 step (its dF is an FP64 residual minus an FP32 one) is not stored
-// (precision_changed).
+// max(1e-5, 100 tolf), or once it has not improved for two steps (the FP32 floor reached,
+// whatever its level: steps spent on it are wasted). An FP32 step whose max|F| is already
+// below tolf is redone in FP64 first, so that it cannot end the solve: convergence
+// (max|F| < tolf) is always decided on an FP64 residual, and the converged state meets the
+// FP64 solve's criterion. At the first FP64 step the Broyden history restarts from the
+// FP32 phase's iterate (precision_changed): its pairs model the FP32 residual function.
 struct Residual2 : BroydenResidual {
     qs_handle *h;
     double V;
@@ -333,7 +333,7 @@ struct Residual2 : BroydenResidual {
             since_best++;
         }
         n_mixed++;
-        if (fmax < h->mixed_switch || since_best >= 5) {
+        if (fmax < h->mixed_switch || since_best >= 2) {
             fp32 = false;  // the next steps are FP64
             if (fmax < h->tolf) {  // never let an FP32 residual declare convergence: redo it
                 n_mixed--;
