@@ -770,7 +770,9 @@ def main():
                     help="1: time kernel variants per size (default); 2/3: force variant 1/2 (profiling only)")
     ap.add_argument("--serve", type=int, default=16,
                     help="requests of the serving stream (0: none; the full stream is 512)")
-    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-rate", type=float, default=0.15,
+                    help="Poisson arrivals per second (0.15: below the ~0.2/s the device serves with 4 solves in "
+                         "flight, so the latencies are service times, not a growing queue)")
     ap.add_argument("--serve-inflight", type=int, default=4, help="solves on the device at once")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="both: the FP64 form (headline value), then the mixed form, with their ratio")

@@ -137,8 +137,48 @@ __device__ __forceinline__ void hist_elem(double f, double fo, double xx, double
     }
 }
 
-template <typename HT, int NH>
-__global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
+// Four elements per thread (16-byte accesses). The NH column loads of a step are issued
+// together, before the dots that use them, so that a step keeps all its loads in flight;
+// the 2 NH FP64 accumulators and those loads need more than 128 registers a thread for
+// NH >= 8, so the long-history forms run one block of 8 warps per SM (still ~80 KB of loads
+// in flight per SM, above what HBM latency asks for).
+template <typename HT, int E> struct HV;
+template <> struct HV<float, 4> { using t = float4; };
+template <> struct HV<double, 4> { using t = double4; };
+template <> struct HV<float, 2> { using t = float2; };
+template <> struct HV<double, 2> { using t = double2; };
+template <int E> __device__ __forceinline__ void ldE(const double *p, double (&o)[E]) {
+    if constexpr (E == 4) {
+        double4 v = ld4(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    } else {
+        double2 v = *(const double2 *)p;
+        o[0] = v.x; o[1] = v.y;
+    }
+}
+template <typename HT, int E> __device__ __forceinline__ void hldE(const HT *p, double (&o)[E]) {
+    if constexpr (E == 4) {
+        hld4<HT>(p, o);
+    } else if constexpr (sizeof(HT) == 4) {
+        float2 v = *(const float2 *)p;
+        o[0] = v.x; o[1] = v.y;
+    } else {
+        double2 v = *(const double2 *)p;
+        o[0] = v.x; o[1] = v.y;
+    }
+}
+template <typename HT, int E> __device__ __forceinline__ void hstE(HT *p, const HT (&v)[E]) {
+    if constexpr (E == 4) {
+        hst4<HT>(p, v);
+    } else if constexpr (sizeof(HT) == 4) {
+        *(float2 *)p = float2{v[0], v[1]};
+    } else {
+        *(double2 *)p = double2{v[0], v[1]};
+    }
+}
+
+template <typename HT, int NH, int E = 4>
+__global__ void __launch_bounds__(256, NH >= 8 ? 1 : 2) hist_update(const double *__restrict__ F, const double *__restrict__ Fold,
                                                       const double *__restrict__ x, const double *__restrict__ xold,
                                                       int64_t n, int64_t ld, double fnorm, double alpha,
                                                       HT *__restrict__ dF, HT *__restrict__ U, int slot, int nh,
@@ -148,60 +188,65 @@ __global__ void __launch_bounds__(256, 2) hist_update(const double *__restrict__
 #pragma unroll
     for (int k = 0; k < NH; k++) { g[k] = 0.0; c[k] = 0.0; }
     const double rf = 1.0 / fnorm;
-    const int64_t n4 = n / 4;
+    const int64_t nE = n / E;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n4 + (n - 4 * n4); q += stride) {
-        const bool vec = q < n4;
-        const int64_t i0 = vec ? 4 * q : 4 * n4 + (q - n4);
-        const int cnt = vec ? 4 : 1;
-        double f[4], dn[4];
-        HT dnew[4] = {0, 0, 0, 0}, unew[4];
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nE + (n - E * nE); q += stride) {
+        const bool vec = q < nE;
+        const int64_t i0 = vec ? E * q : E * nE + (q - nE);
+        const int cnt = vec ? E : 1;
+        double f[E], dn[E];
+        HT dnew[E] = {}, unew[E];
         if (vec) {
-            double4 fv = ld4(F + i0);
-            f[0] = fv.x; f[1] = fv.y; f[2] = fv.z; f[3] = fv.w;
+            ldE<E>(F + i0, f);
         } else {
             f[0] = F[i0];
         }
         if (store) {
-            double fo[4], xx[4], xo[4];
+            double fo[E], xx[E], xo[E];
             if (vec) {
-                double4 a = ld4(Fold + i0), b = ld4(x + i0), cc = ld4(xold + i0);
-                fo[0] = a.x; fo[1] = a.y; fo[2] = a.z; fo[3] = a.w;
-                xx[0] = b.x; xx[1] = b.y; xx[2] = b.z; xx[3] = b.w;
-                xo[0] = cc.x; xo[1] = cc.y; xo[2] = cc.z; xo[3] = cc.w;
+                ldE<E>(Fold + i0, fo);
+                ldE<E>(x + i0, xx);
+                ldE<E>(xold + i0, xo);
             } else {
                 fo[0] = Fold[i0]; xx[0] = x[i0]; xo[0] = xold[i0];
             }
 #pragma unroll
-            for (int e = 0; e < 4; e++)
+            for (int e = 0; e < E; e++)
                 if (e < cnt) hist_elem<HT>(f[e], fo[e], xx[e], xo[e], fnorm, rf, alpha, dnew[e], unew[e]);
             if (vec) {
-                hst4<HT>(dF + (int64_t)slot * ld + i0, dnew);
-                hst4<HT>(U + (int64_t)slot * ld + i0, unew);
+                hstE<HT, E>(dF + (int64_t)slot * ld + i0, dnew);
+                hstE<HT, E>(U + (int64_t)slot * ld + i0, unew);
             } else {
                 dF[(int64_t)slot * ld + i0] = dnew[0];
                 U[(int64_t)slot * ld + i0] = unew[0];
             }
         }
 #pragma unroll
-        for (int e = 0; e < 4; e++) dn[e] = (double)dnew[e];
+        for (int e = 0; e < E; e++) dn[e] = (double)dnew[e];
+        // all column loads of the step first (independent, in flight together; kept in the
+        // history's own type until used), then the dots
+        typename HV<HT, E>::t dk[NH];
+#pragma unroll
+        for (int k = 0; k < NH; k++) {
+            if (k < nh && !(store && k == slot)) {
+                if (vec) {
+                    dk[k] = *(const typename HV<HT, E>::t *)(dF + (int64_t)k * ld + i0);
+                } else {
+                    HT *d = (HT *)&dk[k];
+                    d[0] = dF[(int64_t)k * ld + i0];
+                }
+            }
+        }
 #pragma unroll
         for (int k = 0; k < NH; k++) {
             if (k < nh) {
-                double dk[4];
-                if (store && k == slot) {
+                const HT *d = (const HT *)&dk[k];
 #pragma unroll
-                    for (int e = 0; e < 4; e++) dk[e] = dn[e];
-                } else if (vec) {
-                    hld4<HT>(dF + (int64_t)k * ld + i0, dk);
-                } else {
-                    dk[0] = (double)dF[(int64_t)k * ld + i0];
-                }
-#pragma unroll
-                for (int e = 0; e < 4; e++)
+                for (int e = 0; e < E; e++)
                     if (e < cnt) {
-                        g[k] = fma(dk[e], dn[e], g[k]);
-                        c[k] = fma(dk[e], f[e], c[k]);
+                        const double v = (store && k == slot) ? dn[e] : (double)d[e];
+                        g[k] = fma(v, dn[e], g[k]);
+                        c[k] = fma(v, f[e], c[k]);
                     }
             }
         }

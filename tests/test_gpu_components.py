@@ -347,6 +347,12 @@ def test_autotuner_records_a_choice_per_size():
     key = qb.tune_key(56, m.n_omega)
     assert qb.tuned_choice(qb.TUNE_DYSON, key) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, key) in (1, 2)
     s.close()
+    # the FP32 phase of a mixed handle tunes its own Keldysh decision among the 3xTF32
+    # tensor-core kernel (3) and the FP64 ones (1, 2)
+    mx = qb.Solver(m, precision=qb.QS_PREC_MIXED)
+    mx.residual(0.3, mx.initial_vector(0.3))
+    assert qb.tuned_choice(qb.TUNE_KELDYSH32, key) in (1, 2, 3)
+    mx.close()
 
 
 # ---- failure detection: SCF runaway, as scf_residual2 + check_diag_sanity ----
