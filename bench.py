@@ -901,9 +901,13 @@ def main():
         # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
         # on the 120x120 helix: Dyson and Keldysh per energy at 1024 energies
         # (profiles/dyson_bgj_helix120_n1024.md, profiles/keldysh_tc_helix120_n1024.md); the
-        # Broyden kernels per vector element (profiles/broyden_kernels_helix120.md)
+        # Broyden kernels per vector element (profiles/broyden_kernels_helix120_n1024.md)
         traffic_per_unit = {"dyson_gj": ((236.776192e6 + 183.729152e6) / 1024, n),
-                            "keldysh_scf2": ((1064.643e6 + 800.101376e6) / 1024, n)}
+                            "keldysh_scf2": ((1064.643e6 + 800.101376e6) / 1024, n),
+                            # hist_update_split + x_update + vec_norms of one step (history
+                            # full) per SCF-vector element, averaged over the 3 launches
+                            "broyden": ((4.072997376e9 + 0.356998144e9 + 3.539108352e9 + 0.344236544e9
+                                         + 0.707824128e9) / (3 * 14400 * 1024) / 3, nvec)}
         roof = None
         if fam in work and cnt:
             kind, per_launch = work[fam]

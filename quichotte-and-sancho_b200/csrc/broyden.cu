@@ -273,6 +273,115 @@ __global__ void __launch_bounds__(256, NH >= 8 ? 1 : 2) hist_update(const double
     }
 }
 
+// The same step for long histories (NH = 16, 32) with the columns split over SPL = NH / 8
+// adjacent threads: the threads of a group share their four elements (their F, Fold, x,
+// xold loads are the same transactions) and each keeps the dots of 8 columns, so a thread
+// needs 16 accumulators and 8 column loads, two 8-warp blocks fit on an SM, and each
+// thread's loads of a step are all in flight together.
+template <typename HT, int NH>
+__global__ void __launch_bounds__(256, 2) hist_update_split(const double *__restrict__ F, const double *__restrict__ Fold,
+                                                            const double *__restrict__ x,
+                                                            const double *__restrict__ xold, int64_t n, int64_t ld,
+                                                            double fnorm, double alpha, HT *__restrict__ dF,
+                                                            HT *__restrict__ U, int slot, int nh, int store,
+                                                            double *__restrict__ part) {
+    constexpr int CPT = 8, SPL = NH / CPT, E = 4;
+    __shared__ double sh[2 * NH * 8];
+    const int h = threadIdx.x % SPL;  // this thread's column block: columns h CPT .. h CPT + 7
+    double g[CPT], c[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; k++) { g[k] = 0.0; c[k] = 0.0; }
+    const double rf = 1.0 / fnorm;
+    const int64_t nE = n / E;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x / SPL;
+    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / SPL; q < nE + (n - E * nE); q += stride) {
+        const bool vec = q < nE;
+        const int64_t i0 = vec ? E * q : E * nE + (q - nE);
+        const int cnt = vec ? E : 1;
+        double f[E], dn[E];
+        HT dnew[E] = {}, unew[E];
+        if (vec) {
+            ldE<E>(F + i0, f);
+        } else {
+            f[0] = F[i0];
+        }
+        if (store) {
+            double fo[E], xx[E], xo[E];
+            if (vec) {
+                ldE<E>(Fold + i0, fo);
+                ldE<E>(x + i0, xx);
+                ldE<E>(xold + i0, xo);
+            } else {
+                fo[0] = Fold[i0]; xx[0] = x[i0]; xo[0] = xold[i0];
+            }
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                if (e < cnt) hist_elem<HT>(f[e], fo[e], xx[e], xo[e], fnorm, rf, alpha, dnew[e], unew[e]);
+            if (h == 0) {
+                if (vec) {
+                    hstE<HT, E>(dF + (int64_t)slot * ld + i0, dnew);
+                    hstE<HT, E>(U + (int64_t)slot * ld + i0, unew);
+                } else {
+                    dF[(int64_t)slot * ld + i0] = dnew[0];
+                    U[(int64_t)slot * ld + i0] = unew[0];
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) dn[e] = (double)dnew[e];
+        typename HV<HT, E>::t dk[CPT];
+#pragma unroll
+        for (int kk = 0; kk < CPT; kk++) {
+            const int k = h * CPT + kk;
+            if (k < nh && !(store && k == slot)) {
+                if (vec) {
+                    dk[kk] = *(const typename HV<HT, E>::t *)(dF + (int64_t)k * ld + i0);
+                } else {
+                    HT *d = (HT *)&dk[kk];
+                    d[0] = dF[(int64_t)k * ld + i0];
+                }
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < CPT; kk++) {
+            const int k = h * CPT + kk;
+            if (k < nh) {
+                const HT *d = (const HT *)&dk[kk];
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    if (e < cnt) {
+                        const double v = (store && k == slot) ? dn[e] : (double)d[e];
+                        g[kk] = fma(v, dn[e], g[kk]);
+                        c[kk] = fma(v, f[e], c[kk]);
+                    }
+            }
+        }
+    }
+    // sums over the warp's lanes of the same column block (lanes h, h + SPL, ...), then over
+    // the block's warps
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int kk = 0; kk < CPT; kk++) {
+        double a = g[kk], b = c[kk];
+#pragma unroll
+        for (int o = 16; o >= SPL; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane < SPL) {
+            const int k = lane * CPT + kk;
+            sh[(2 * k) * 8 + wid] = a;
+            sh[(2 * k + 1) * 8 + wid] = b;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * nh; t += blockDim.x) {
+        double s2 = 0.0;
+        for (int w = 0; w < nw; w++) s2 += sh[t * 8 + w];
+        part[(int64_t)blockIdx.x * 2 * MAXH + t] = s2;
+    }
+}
+
 template <typename HT>
 static void launch_hist(int nb, cudaStream_t st, const double *F, const double *Fold, const double *x, const double *xold,
                         int64_t n, double fnorm, double alpha, HT *dF, HT *U, int slot, int nh, int store, double *part) {
@@ -282,9 +391,11 @@ static void launch_hist(int nb, cudaStream_t st, const double *F, const double *
     else if (nh <= 8)
         hist_update<HT, 8><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
     else if (nh <= 16)
-        hist_update<HT, 16><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update_split<HT, 16><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh,
+                                                               store, part);
     else
-        hist_update<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh, store, part);
+        hist_update_split<HT, 32><<<nb, RED_THREADS, 0, st>>>(F, Fold, x, xold, n, ld, fnorm, alpha, dF, U, slot, nh,
+                                                               store, part);
 }
 
 // x_new = x + alpha F - sum_k gamma_k U_k   (common/broyden_mixing.f90:165-178), the
