@@ -140,12 +140,13 @@ BROYDEN = dict(alpha_mix=0.5, nhist=16, tolf=1e-6, maxscf=300, single_history=1)
 SAMPLE_N = 1024
 # SCF iterations per voltage of this sweep in the FP64 form on B200 (all 41 voltages, swept
 # -1 -> 1 V with continuation, fresh after an unconverged voltage, maxscf 300; one B200, the
-# default Broyden settings); 300 marks a voltage that did not converge. The CPU arm multiplies
+# default Broyden settings; -0.75 ... +0.20 V from the bench's own run with 5 warm-up and 20
+# timed points); 300 marks a voltage that did not converge. The CPU arm multiplies
 # its measured time per iteration by this work (the oracle runs the same algorithm, so the same
 # iterations).
-SWEEP_ITERS_B200 = dict(zip(VOLTS, [32, 27, 27, 26, 25, 25, 24, 23, 22, 21, 20, 19, 18, 16, 19, 18, 24, 24, 228,
-                                    300, 300, 300, 300, 300, 300, 300, 210, 16, 18, 20, 23, 25, 26, 27, 28, 27,
-                                    28, 29, 30, 30, 31]))
+SWEEP_ITERS_B200 = dict(zip(VOLTS, [32, 27, 27, 26, 25, 25, 24, 23, 22, 21, 20, 19, 18, 16, 19, 19, 24, 24, 183, 300,
+                                    300, 300, 300, 300, 300, 300, 210, 16, 18, 20, 23, 25, 26, 27, 28, 27, 28, 29,
+                                    30, 30, 31]))
 
 
 def bench_config(n_omega, ions, turns, nhist, world):
