@@ -223,14 +223,17 @@ void qs_server_destroy(qs_server *s);
 
 /* ---- autotuner (no counterpart in the reference) ----
  * Kernel variants whose relative speed depends on the size (kind 0: Dyson, blocked tensor-
- * core or unblocked Gauss-Jordan; kind 1: Keldysh, tensor-core or CUDA-core GEMMs; kinds 2
+ * core (variant 1: in shared memory, one block per SM, or in the global workspace above the
+ * shared-memory limit; variant 3: in the global workspace, two blocks per SM) or unblocked
+ * Gauss-Jordan (2); kind 1: Keldysh, tensor-core or CUDA-core GEMMs; kinds 2
  * and 3: the tile width 4 or 2 of the persistent Sigma2 kernels A and C, +2^20 in the key
  * for the FP32 ones; kind 4: the Keldysh step of a mixed solve's FP32 phase, variant 3 the
  * 3xTF32 kernel on the fifth-generation tensor cores, 1 / 2 the FP64 ones) are timed on the
  * first launch at a new size and the fastest is kept for the process.
  * qs_autotune(1) tunes (default), qs_autotune(0) uses the size heuristics only, 2 / 3 force
  * the first (kind 4: the 3xTF32 kernel; else the tensor-core / blocked variant) / last
- * applicable variant, qs_autotune(-1) forgets the recorded choices. qs_tuned_choice returns
+ * applicable variant, 4 the second of three (kind 0: variant 3; kind 4: the FP64 tensor-core
+ * kernel), qs_autotune(-1) forgets the recorded choices. qs_tuned_choice returns
  * the recorded variant (1, 2 or 3) or -1; a decision
  * is keyed by size = order + 1024 * floor(log2(n_omega)) (order N for Dyson, nA for Keldysh). */
 int qs_autotune(int mode);

@@ -18,8 +18,8 @@ namespace qs {
 
 static std::mutex g_tune_mu;
 static std::map<std::pair<int, int>, int> g_tune;
-// 1: tune; 0: the size heuristics only; 2 / 3: the first / last applicable candidate
-// (tests force each variant this way)
+// 1: tune; 0: the size heuristics only; 2 / 3: the first / last applicable candidate; 4: the
+// second of three (tests force each variant this way)
 static int g_tune_mode = 1;
 
 static int tune_mode() {
@@ -48,6 +48,7 @@ int tune_launch(qs_handle *h, int kind, int size, const int *cand, int ncand, in
                 const std::function<int(int)> &launch) {
     const int mode = tune_mode();
     if (mode == 2 || mode == 3) return launch(cand[mode == 2 ? 0 : ncand - 1]);
+    if (mode == 4) return launch(cand[ncand >= 3 ? 1 : 0]);
     if (ncand <= 1 || mode == 0) return launch(ncand == 1 ? cand[0] : fallback);
     const int known = tune_get(kind, size);
     if (known >= 0) return launch(known);
@@ -90,7 +91,7 @@ extern "C" {
 int qs_autotune(int mode) {
     std::lock_guard<std::mutex> lk(qs::g_tune_mu);
     if (mode < 0) qs::g_tune.clear();
-    else if (mode <= 3) qs::g_tune_mode = mode;
+    else if (mode <= 4) qs::g_tune_mode = mode;
     else return -1;
     return 0;
 }

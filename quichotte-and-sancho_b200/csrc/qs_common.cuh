@@ -259,7 +259,9 @@ int sigma2_compute(qs_handle *h, const double *d_x, bool fp32 = false);
 // TUNE_KELDYSH32: the Keldysh step of a mixed solve's FP32 phase, where the 3xTF32 tensor-core
 // kernel (keldysh_tf32.cu) competes with the two FP64 ones
 enum TuneKind { TUNE_DYSON = 0, TUNE_KELDYSH = 1, TUNE_SIG2_A = 2, TUNE_SIG2_C = 3, TUNE_KELDYSH32 = 4 };
-enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, KELDYSH_TC = 1, KELDYSH_CUDA = 2, KELDYSH_TF32 = 3 };
+// DYSON_BLOCKED2: the blocked Gauss-Jordan with its matrix in the global workspace, two
+// 8-warp blocks per SM
+enum { DYSON_BLOCKED = 1, DYSON_UNBLOCKED = 2, DYSON_BLOCKED2 = 3, KELDYSH_TC = 1, KELDYSH_CUDA = 2, KELDYSH_TF32 = 3 };
 // the size key of a decision: the matrix order and the octave of the grid length (how many
 // energies each SM gets changes which variant wins)
 inline int tune_key(int order, int n) {

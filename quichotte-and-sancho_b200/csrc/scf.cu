@@ -562,7 +562,7 @@ static size_t handle_need(const qs_handle *h) {
     need += (size_t)n * (4 * h->N_sites * zc_ + N * 8 + 16);                // onsL, dosd, trU, trD
     if (h->has_atomL) need += (size_t)n * h->atom_off.back() * zc_;
     need += (size_t)n * std::max(nA, 1) * zc_ * 2;                           // gRd, gLd
-    if (!dyson_fits_smem(N)) need += (size_t)148 * 2 * nn * zc_;            // Gauss-Jordan workspace
+    if (!dyson_fits_smem(N) || (N > 16 && N <= 256)) need += (size_t)148 * 2 * nn * zc_;  // Gauss-Jordan workspace
     if (h->order == 2) {
         size_t nY = (size_t)nA * nA + (size_t)nA * (nA + 1) / 2;
         need += (size_t)h->n_vec * 8 * 4;                                     // x, F, Fold, xold
@@ -660,8 +660,9 @@ int qs_create(const qs_problem *p, qs_handle **out) {
     if ((rc = dalloc(h, (void **)&h->d_info, sizeof(int) * 2))) return rc;
     int imax = INT_MAX;
     QS_CUDA(h, cudaMemcpyAsync(h->d_info, &imax, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    // Gauss-Jordan workspace for matrices that do not fit in shared memory
-    if (!dyson_fits_smem(N)) {
+    // Gauss-Jordan workspace: for matrices that do not fit in shared memory, and for the
+    // two-blocks-per-SM blocked variant (16 < N <= 256)
+    if (!dyson_fits_smem(N) || (N > 16 && N <= 256)) {
         h->ws_slots = 148 * 2;
         if ((rc = dalloc(h, (void **)&h->d_Gws, h->ws_slots * nn * zc_))) return rc;
     }

@@ -243,8 +243,10 @@ constexpr int BGJ_MAXN_GM = 256;
 //           tensor cores; the warp reads its A[K, j] fragment before it rewrites those rows,
 //           so no block barrier separates the two
 // The row interchanges are undone by column interchanges in reverse order at the end.
-template <bool GM>
-__global__ void __launch_bounds__(BGJ_THREADS) dyson_bgj_t(DysonArgs a) {
+// NT = 480 (15 warps, one block per SM) or, with the matrix in the global workspace, NT = 256
+// (8 warps, two blocks per SM: one block's latency-bound panel overlaps the other's update).
+template <bool GM, int NT = BGJ_THREADS>
+__global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) dyson_bgj_t(DysonArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int PWM = GM ? 8 : 4;  // panel warps at most
     const int N = a.N;
@@ -1080,9 +1082,23 @@ static bool use_blocked(int N) { return N >= 16 && N <= 128 && (size_t)swz_units
 // limit up to 256
 static bool use_blocked_gm(int N) { return !use_blocked(N) && N > 16 && N <= BGJ_MAXN_GM; }
 static inline auto dyson_bgj = dyson_bgj_t<false>;
+constexpr int BGJ_THREADS2 = 256;  // the two-blocks-per-SM form (workspace)
+// the workspace form runs for 16 < N <= 256 (also below the shared-memory limit, as the
+// two-blocks-per-SM variant of the tuner)
+static bool use_bgj_ws(int N) { return N > 16 && N <= BGJ_MAXN_GM; }
 
 static int launch_dyson(qs_handle *h, DysonArgs &a, int nblocks, int variant) {
     const int N = a.N;
+    if (variant == DYSON_BLOCKED2 && use_bgj_ws(N) && h->d_Gws) {
+        // two blocks of 8 warps per SM, each matrix in its block's slot of the workspace
+        a.ws = h->d_Gws;
+        nblocks = std::min<int>(std::min(nblocks, 2 * 148), (int)h->ws_slots);
+        int pi = prof_begin(h, K_DYSON);
+        dyson_bgj_t<true, BGJ_THREADS2><<<nblocks, BGJ_THREADS2, 0, h->stream>>>(a);
+        prof_end(h, pi);
+        QS_CUDA(h, cudaGetLastError());
+        return 0;
+    }
     if (variant == DYSON_BLOCKED && use_blocked_gm(N) && h->d_Gws) {
         // one block per SM: the concurrent matrices (148 x N^2 x 16 B) stay mostly in L2
         a.ws = h->d_Gws;
@@ -1210,9 +1226,11 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         a.out_mode = 0;
         a.Gout = h->d_G;
         {
-            const int cand[2] = {DYSON_BLOCKED, DYSON_UNBLOCKED};
-            const bool two = use_blocked(N) || (use_blocked_gm(N) && h->d_Gws);
-            rc = tune_launch(h, TUNE_DYSON, tune_key(N, n), two ? cand : cand + 1, two ? 2 : 1, DYSON_BLOCKED,
+            int cand[3], nc = 0;
+            if (use_blocked(N) || (use_blocked_gm(N) && h->d_Gws)) cand[nc++] = DYSON_BLOCKED;
+            if (use_bgj_ws(N) && h->d_Gws) cand[nc++] = DYSON_BLOCKED2;
+            cand[nc++] = DYSON_UNBLOCKED;
+            rc = tune_launch(h, TUNE_DYSON, tune_key(N, n), cand, nc, nc > 1 ? cand[0] : DYSON_UNBLOCKED,
                              [&](int v) { return launch_dyson(h, a, std::min(n, 148 * 16), v); });
             if (rc) return rc;
         }

@@ -182,8 +182,9 @@ _lib.qs_tuned_choice.argtypes = [ctypes.c_int, ctypes.c_int]
 
 
 def autotune(mode):
-    """1: time kernel variants per size (default); 0: size heuristics; 2/3: force variant
-    1 (tensor-core/blocked) or 2; -1: forget the recorded choices."""
+    """1: time kernel variants per size (default); 0: size heuristics; 2/3: force the first
+    (tensor-core/blocked) or last variant; 4: the second of three (the two-blocks-per-SM
+    blocked Dyson); -1: forget the recorded choices."""
     if _lib.qs_autotune(mode) != 0:
         raise ValueError(mode)
 

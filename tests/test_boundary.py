@@ -63,7 +63,7 @@ def test_memory_estimate_grows_with_the_problem_and_needs_no_device():
 
 
 def test_autotune_modes_are_checked():
-    for mode in (-1, 0, 1, 2, 3):
+    for mode in (-1, 0, 1, 2, 3, 4):
         qb.autotune(mode)
     qb.autotune(1)
     with pytest.raises(ValueError):

@@ -293,11 +293,12 @@ def test_mixed_solve_matches_fp64_solve(case):
 
 # ---- autotuner: every variant it chooses between computes the same step ----
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", [2, 3, 4])
 @pytest.mark.parametrize("ions_turns", [(4, 2), (7, 4), (10, 6)])
 def test_forced_kernel_variants_match_oracle(mode, ions_turns):
-    """Blocked/tensor-core (mode 2) and unblocked/CUDA-core (mode 3) Dyson and Keldysh at
-    N = nA = 16, 56, 120: residual within 1e-11 of the oracle."""
+    """Blocked/tensor-core (mode 2), unblocked/CUDA-core (mode 3) and the blocked Dyson on the
+    global workspace with two blocks per SM (mode 4, N > 16) at N = nA = 16, 56, 120:
+    residual within 1e-11 of the oracle."""
     ni, nt = ions_turns
     m = qb.Model.helix(N_ions=ni, N_turns=nt, hel_length=0.34 * nt, hel_radius=0.7, hand=1.0, E_CC=0.0, t_hop=1.0,
                        lamb=0.01, U_int=1.0, GammaL_up=0.5, GammaL_down=0.5, GammaR=0.5, T=300.0, mu=0.0,
@@ -313,7 +314,7 @@ def test_forced_kernel_variants_match_oracle(mode, ions_turns):
         qb.autotune(1)
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", [2, 3, 4])
 @pytest.mark.parametrize("ions_turns", [(17, 4), (16, 6)])
 def test_dyson_above_shared_memory_matches_oracle(mode, ions_turns):
     """N = 136, 192: the matrix no longer fits in shared memory. Mode 2 forces the blocked
@@ -345,7 +346,7 @@ def test_autotuner_records_a_choice_per_size():
     s.residual(0.3, s.initial_vector(0.3))
     assert s.nA == 56
     key = qb.tune_key(56, m.n_omega)
-    assert qb.tuned_choice(qb.TUNE_DYSON, key) in (1, 2) and qb.tuned_choice(qb.TUNE_KELDYSH, key) in (1, 2)
+    assert qb.tuned_choice(qb.TUNE_DYSON, key) in (1, 2, 3) and qb.tuned_choice(qb.TUNE_KELDYSH, key) in (1, 2)
     s.close()
     # the FP32 phase of a mixed handle tunes its own Keldysh decision among the 3xTF32
     # tensor-core kernel (3) and the FP64 ones (1, 2)
