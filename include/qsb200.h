@@ -242,8 +242,14 @@ int qs_tuned_choice(int kind, int size);
 /* ---- instrumentation (no counterpart in the reference, whose only timer is the
  * wall clock of src/quichotte.f90:50-58) ---- */
 
-/* Number of kernels this library has launched in the process so far. */
+/* Number of kernels this library has launched in the process so far (the kernels of a
+ * replayed CUDA graph included). */
 int64_t qs_kernel_launches(void);
+
+/* SCF residuals of this handle replayed from a CUDA graph: the FP64 residual's launches
+ * (G^<(t=0), Sigma2, Dyson, Keldysh, the sanity sums) are captured once per (x, F, V) buffer
+ * pair and replayed by the Broyden loop (not while per-launch profiling is on). */
+int64_t qs_graph_replays(const qs_handle *h);
 
 /* Per-kernel-family device time measured with CUDA events on the solver's stream.
  * enable = 1 starts recording, 0 stops, -1 only reads and resets. Fills ms[f] and

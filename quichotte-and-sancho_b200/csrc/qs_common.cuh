@@ -193,6 +193,19 @@ struct qs_handle {
     std::string err;
     size_t bytes_allocated = 0;
     std::vector<void *> allocs;
+    // CUDA graphs of the FP64 residual's launches, one per (x, F, V) the Broyden loop uses
+    // (x and F alternate between two buffers each): replayed instead of re-launching
+    struct ResidualGraph {
+        const double *x = nullptr;
+        double *F = nullptr;
+        double V = 0.0;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;  // kernels in the graph (added to the launch count per replay)
+    };
+    ResidualGraph graphs[2];
+    int graph_next = 0;
+    bool graphs_off = false;   // a capture failed: eager launches from then on
+    int64_t graph_replays = 0;
 };
 
 namespace qs {
@@ -221,6 +234,7 @@ inline cudaError_t smem_cap(const void *kernel) {
 
 // every kernel launch of the library is counted (qs_kernel_launches)
 void count_launch();
+void count_launches(int64_t k);
 // bracket a launch with events when profiling is on: idx = prof_begin(...); launch; prof_end(h, idx)
 int prof_begin(qs_handle *h, int fam, bool count = true);
 void prof_end(qs_handle *h, int idx);

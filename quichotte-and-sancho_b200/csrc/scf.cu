@@ -26,6 +26,7 @@ size_t broyden_red_len();
 
 static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 int prof_begin(qs_handle *h, int fam, bool count) {
     if (count) count_launch();
@@ -193,21 +194,28 @@ int read_info(qs_handle *h, int &info) {
     return 0;
 }
 
-// sums over energies of the diagonals gRd, gLd -> sanity of the active states
-int sweep_sanity(qs_handle *h, SanityOut &s) {
-    zc *sums = (zc *)h->d_red;  // [nA] gLd sums, then [nA] gRd sums
-    int rc;
-    if ((rc = sum_over_energies(h, h->d_gLd, h->nA, h->nA, h->n, sums))) return rc;
-    if ((rc = sum_over_energies(h, h->d_gRd, h->nA, h->nA, h->n, sums + h->nA))) return rc;
+// the sanity of the active states from the sums over energies of the diagonals gRd, gLd
+// already formed in the reduction scratch ([nA] gLd sums, then [nA] gRd sums)
+int sweep_sanity_read(qs_handle *h, SanityOut &s) {
+    zc *sums = (zc *)h->d_red;
     std::vector<zc> hs(2 * h->nA);
     QS_CUDA(h, cudaMemcpyAsync(hs.data(), sums, sizeof(zc) * 2 * h->nA, cudaMemcpyDeviceToHost, h->stream));
-    int info;
+    int info, rc;
     if ((rc = read_info(h, info))) return rc;
     std::vector<zc> sl(hs.begin(), hs.begin() + h->nA);
     std::vector<double> sr(h->nA);
     for (int i = 0; i < h->nA; i++) sr[i] = hs[h->nA + i].y;
     s = check_diag_sanity(h->nA, sl, sr, h->delta, h->act.data());
     return 0;
+}
+
+// sums over energies of the diagonals gRd, gLd -> sanity of the active states
+int sweep_sanity(qs_handle *h, SanityOut &s) {
+    zc *sums = (zc *)h->d_red;  // [nA] gLd sums, then [nA] gRd sums
+    int rc;
+    if ((rc = sum_over_energies(h, h->d_gLd, h->nA, h->nA, h->n, sums))) return rc;
+    if ((rc = sum_over_energies(h, h->d_gRd, h->nA, h->nA, h->n, sums + h->nA))) return rc;
+    return sweep_sanity_read(h, s);
 }
 
 // order-1 vector: Re, Im of the 2x2 on-site block of G^<(t=0) of each interacting site
@@ -295,6 +303,65 @@ int onsite_sums(qs_handle *h, std::vector<zc> &sums) {
 // (max|F| < tolf) is always decided on an FP64 residual, and the converged state meets the
 // FP64 solve's criterion. At the first FP64 step the Broyden history restarts from the
 // FP32 phase's iterate (precision_changed): its pairs model the FP32 residual function.
+// The device work of one order-2 residual: G^<(t=0) and Sigma1, Sigma2, the sweep writing
+// F = pack(G_out) - x, the sanity sums (no host synchronisation in between).
+int residual2_launches(qs_handle *h, double V, const double *d_x, double *d_F, bool use32) {
+    int rc;
+    if ((rc = equal_time_lesser_sigma1(h, d_x))) return rc;
+    if ((rc = sigma2_compute(h, d_x, use32))) return rc;
+    if ((rc = sweep(h, M_SCF2, V, true, d_F, d_x, use32))) return rc;
+    zc *sums = (zc *)h->d_red;
+    if ((rc = sum_over_energies(h, h->d_gLd, h->nA, h->nA, h->n, sums))) return rc;
+    if ((rc = sum_over_energies(h, h->d_gRd, h->nA, h->nA, h->n, sums + h->nA))) return rc;
+    return 0;
+}
+
+// The FP64 residual's launches replayed from a CUDA graph: captured at the second evaluation
+// of an (x, F, V) (the first one has made every autotuner decision of the sizes), replayed
+// afterwards. Not with per-launch profiling on (its events are per launch) nor in the FP32
+// phase; a capture that fails turns graphs off for the handle (eager launches, same results).
+int residual2_graphed(qs_handle *h, double V, const double *d_x, double *d_F) {
+    for (auto &g : h->graphs)
+        if (g.exec && g.x == d_x && g.F == d_F && g.V == V) {
+            QS_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+            count_launches(g.launches);
+            h->graph_replays++;
+            return 0;
+        }
+    auto &g = h->graphs[h->graph_next];
+    h->graph_next ^= 1;
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    const int64_t l0 = qs_kernel_launches();
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        h->graphs_off = true;
+        return residual2_launches(h, V, d_x, d_F, false);
+    }
+    int rc = residual2_launches(h, V, d_x, d_F, false);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    const int64_t captured = qs_kernel_launches() - l0;
+    if (rc == 0 && e == cudaSuccess && graph) e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != 0 || e != cudaSuccess || !g.exec) {
+        cudaGetLastError();  // the failed capture leaves nothing behind on the stream
+        g.exec = nullptr;
+        h->graphs_off = true;
+        h->err.clear();
+        return residual2_launches(h, V, d_x, d_F, false);
+    }
+    g.x = d_x;
+    g.F = d_F;
+    g.V = V;
+    g.launches = captured;
+    QS_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+    h->graph_replays++;
+    return 0;
+}
+
 struct Residual2 : BroydenResidual {
     qs_handle *h;
     double V;
@@ -304,14 +371,19 @@ struct Residual2 : BroydenResidual {
     double best = HUGE_VAL;
     int since_best = 0;
     int last_prec = -1, cur_prec = -1;  // 1 = FP32 phase, 0 = FP64, of the last two evaluations
+    int evals64 = 0;                    // FP64 evaluations of this solve (the first runs eagerly)
     bool precision_changed() const override { return last_prec >= 0 && last_prec != cur_prec; }
     int eval(const double *d_x, double *d_F, bool &abort, bool use32) {
         int rc;
-        if ((rc = equal_time_lesser_sigma1(h, d_x))) return rc;
-        if ((rc = sigma2_compute(h, d_x, use32))) return rc;
-        if ((rc = sweep(h, M_SCF2, V, true, d_F, d_x, use32))) return rc;
+        const bool graph = !use32 && !h->prof_on && !h->graphs_off && evals64 > 0;
+        if (!use32) evals64++;
+        if (graph) {
+            if ((rc = residual2_graphed(h, V, d_x, d_F))) return rc;
+        } else if ((rc = residual2_launches(h, V, d_x, d_F, use32))) {
+            return rc;
+        }
         SanityOut s;
-        if ((rc = sweep_sanity(h, s))) return rc;
+        if ((rc = sweep_sanity_read(h, s))) return rc;
         abort = s.runaway;
         if (abort) QS_CUDA(h, cudaMemsetAsync(d_F, 0, sizeof(double) * h->n_vec, h->stream));
         return 0;
@@ -705,6 +777,8 @@ int qs_create(const qs_problem *p, qs_handle **out) {
 void qs_destroy(qs_handle *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto &g : h->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     release_all(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -727,6 +801,7 @@ int qs_estimate_bytes(const qs_problem *p, double *gib) {
 double qs_device_bytes(const qs_handle *h) { return h ? (double)h->bytes_allocated / (double)(1ull << 30) : 0.0; }
 
 int64_t qs_kernel_launches(void) { return g_launches.load(); }
+int64_t qs_graph_replays(const qs_handle *h) { return h ? h->graph_replays : -1; }
 
 int qs_profile(qs_handle *h, int enable, double *ms, int64_t *launches, int nfam) {
     QS_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -145,6 +145,8 @@ def bind_solver(lib, prefix):
 
 bind_solver(_lib, "qs_")
 _lib.qs_kernel_launches.restype = ctypes.c_int64
+_lib.qs_graph_replays.argtypes = [ctypes.c_void_p]
+_lib.qs_graph_replays.restype = ctypes.c_int64
 _lib.qs_profile.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
 KERNEL_FAMILIES = ("dyson_gj", "keldysh_scf2", "sig2_fwdA", "sig2_mid", "sig2_invC", "final_outputs", "broyden",
                    "reductions", "other")
@@ -158,7 +160,7 @@ def kernel_launches():
 C_ABI = ("qs_create", "qs_destroy", "qs_last_error", "qs_solve_scf", "qs_current", "qs_get_observables",
          "qs_vector_length", "qs_active_states", "qs_fft_length", "qs_initial_vector", "qs_residual",
          "qs_self_energies", "qs_invert_batched", "qs_pack_gf", "qs_unpack_gf", "qs_broyden_solve_host",
-         "qs_kernel_launches", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
+         "qs_kernel_launches", "qs_graph_replays", "qs_profile", "qs_invert_batched_noalloc", "qs_estimate_bytes", "qs_device_bytes",
          "qs_server_create", "qs_server_submit", "qs_server_poll", "qs_server_pending", "qs_server_clock",
          "qs_server_budget_gib", "qs_server_destroy", "qs_autotune", "qs_tuned_choice",
          "qs_hermitian_eigensystem", "qs_hermitian_eigenvalues", "qs_dftb_lowdin")
@@ -339,6 +341,10 @@ class Solver:
 
     def __del__(self):
         self.close()
+
+    def graph_replays(self):
+        """SCF residuals of this handle replayed from a CUDA graph (qs_graph_replays)."""
+        return int(self.lib.qs_graph_replays(self._h)) if self.prefix == "qs_" else 0
 
     def device_gib(self):
         """Device memory (GiB) this handle has allocated."""

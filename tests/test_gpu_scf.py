@@ -43,3 +43,28 @@ def test_solve_scf_matches_oracle_to_1e10(case):
         for key in ("G_less_obs", "dosd"):
             err = np.max(np.abs(og[key] - oo[key])) / np.max(np.abs(oo[key]))
             assert err < 1e-10, (key, err)
+
+
+@pytest.mark.parametrize("case", ["order2_second_order", "order2_dftb_hs"])
+def test_graph_replayed_residuals_equal_eager_ones(case):
+    """The FP64 Broyden loop replays each residual's launches from a CUDA graph (captured once
+    per (x, F, V) buffer pair). The same sweep with per-launch profiling on runs every launch
+    eagerly: both take the same steps and give bit-identical currents and observables, and
+    both count the same kernel launches."""
+    m = qb.Model.load(os.path.join(g.GOLDEN, "cases", case))
+    a, b = qb.Solver(m), qb.Solver(m)
+    b.profile(True)
+    for k, V in enumerate([m.V, m.V + 0.1]):
+        l0 = qb.kernel_launches()
+        ra = a.solve_scf(V, k == 0)
+        la = qb.kernel_launches() - l0
+        l0 = qb.kernel_launches()
+        rb = b.solve_scf(V, k == 0)
+        lb = qb.kernel_launches() - l0
+        assert (ra["converged"], ra["n_iter"]) == (rb["converged"], rb["n_iter"])
+        assert la == lb
+        assert a.current(V) == b.current(V)
+        oa, ob = a.observables(), b.observables()
+        for key in oa:
+            assert np.array_equal(oa[key], ob[key]), key
+    assert a.graph_replays() > 0 and b.graph_replays() == 0
