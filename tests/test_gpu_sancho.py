@@ -148,3 +148,26 @@ def test_program_matches_oracle_program_on_a_finer_grid(tmp_path):
     for f in ("Volt_Current_3.dat", "populations.dat", "spectral_function.dat"):
         ok, worst, msg = g.compare_files(os.path.join(dg, f), os.path.join(do, f))
         assert ok, msg
+
+
+def test_site_dependent_u_and_no_continuation_match_oracle(tmp_path):
+    """hubbard_file (one U per site, setup_hubbard, SANCHO/src/input_output.f90:106-132) with
+    a site at U = 0, and continuation = F (every voltage from the non-interacting start):
+    the program's output files equal the oracle program's."""
+    d = case_dir(str(tmp_path), "u", order=3, N_sites=5, delta=0.005, hubbard_file="U.dat", continuation="F",
+                 V=-0.3, Vf=0.3, delv=0.3)
+    with open(os.path.join(d, "U.dat"), "w") as f:
+        f.write("0.9\n0.0\n0.6\n1.1\n0.4\n")
+    dg, do = str(tmp_path / "gpu"), str(tmp_path / "cpu")
+    shutil.copytree(d, dg)
+    shutil.copytree(d, do)
+    assert sb.run_program(dg) == 0
+    import subprocess
+    with open(os.path.join(do, "stdout.txt"), "w") as out:
+        assert subprocess.run([oracle_lib.SANCHO_ORACLE_EXE, do], stdout=out, stderr=subprocess.STDOUT,
+                              timeout=900).returncode == 0
+    for f in ("Volt_Current_3.dat", "populations.dat", "spectral_function.dat"):
+        ok, worst, msg = g.compare_files(os.path.join(dg, f), os.path.join(do, f))
+        assert ok, msg
+    m = sb.SanchoModel.load(d)
+    assert list(m.U_site) == [0.9, 0.0, 0.6, 1.1, 0.4] and not m.continuation
