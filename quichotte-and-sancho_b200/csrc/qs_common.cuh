@@ -154,6 +154,8 @@ struct qs_handle {
     // device model arrays
     qs::zc *d_Hemb = nullptr, *d_Sig1 = nullptr, *d_GamLs = nullptr, *d_GamRs = nullptr, *d_GamLcl = nullptr;
     int *d_pos = nullptr;
+    int *d_kd_cidx = nullptr;  // contact states of GamLs / GamRs (the lead terms of SL)
+    int kd_nc = -1;
     int *d_act = nullptr, *d_sup = nullptr, *d_cl = nullptr, *d_atom_first = nullptr, *d_atom_norb = nullptr,
         *d_atom_off = nullptr, *d_site_int = nullptr;
     double *d_omega = nullptr, *d_U = nullptr;
@@ -259,6 +261,8 @@ struct KeldyshArgs {
     zc *gRd, *gLd;      // diagonals, or nullptr
     zc *Tws;            // per-block scratch, nA^2 complex
     int *err;           // set to 1 if a bounded tensor-core wait gave up (tcgen05 kernel)
+    const int *cidx;    // the contact states: rows/columns where GamLs or GamRs is non-zero
+    int nc;             // their number (-1: not known)
 };
 // the FP32-phase Keldysh step of a QS_PREC_MIXED solve on the fifth-generation tensor cores
 // (keldysh_tf32.cu): 32 <= nA <= 128; returns -1 for other sizes

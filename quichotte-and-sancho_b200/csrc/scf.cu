@@ -709,7 +709,22 @@ int qs_create(const qs_problem *p, qs_handle **out) {
             GLcl[a + (size_t)b * h->nCL] = zc{h->GammaL[2 * k], h->GammaL[2 * k + 1]};
         }
     std::vector<int> site_int(h->site_int.begin(), h->site_int.end());
+    // the contact states: the rows and columns where the lead matrices are non-zero (the
+    // Keldysh kernel adds their term to T = G Sigma2^< as a low-rank correction)
+    std::vector<int> cidx;
+    for (int k = 0; k < nS; k++) {
+        bool nz = false;
+        for (int j = 0; j < nS && !nz; j++) {
+            const size_t kj = k + (size_t)j * nS, jk = j + (size_t)k * nS;
+            nz = GLs[kj].x != 0.0 || GLs[kj].y != 0.0 || GRs[kj].x != 0.0 || GRs[kj].y != 0.0 || GLs[jk].x != 0.0 ||
+                 GLs[jk].y != 0.0 || GRs[jk].x != 0.0 || GRs[jk].y != 0.0;
+        }
+        if (nz) cidx.push_back(k);
+    }
+    h->kd_nc = (int)cidx.size();
+    if (cidx.empty()) cidx.push_back(0);
     int rc;
+    if ((rc = upload(h, &h->d_kd_cidx, cidx))) return rc;
     if ((rc = upload(h, &h->d_Hemb, Hemb)) || (rc = dalloc(h, (void **)&h->d_Sig1, nn * zc_)) ||
         (rc = upload(h, &h->d_GamLs, GLs)) || (rc = upload(h, &h->d_GamRs, GRs)) || (rc = upload(h, &h->d_GamLcl, GLcl)) ||
         (rc = upload(h, &h->d_pos, h->pos)) || (rc = upload(h, &h->d_act, h->act)) || (rc = upload(h, &h->d_sup, h->sup)) ||

@@ -701,6 +701,7 @@ __device__ __forceinline__ void kd_gemm(const zc *__restrict__ A, const zc *__re
 // s < 8, so the warps share every pass evenly. Operand panels as in kd_gemm (B conjugate-
 // transposed from G); put(i, j, re, im) receives every element of the warp's tiles.
 constexpr int KD_SLOTS = 8;
+constexpr int KD_NCMAX = 16;  // contact states up to which the lead term is a low-rank correction
 __device__ __forceinline__ int kd_upper_tiles(int nA) {
     int cnt = 0;
     for (int ct = 0; 8 * ct < nA; ct++) cnt += min((8 * ct + 7) / 16 + 1, (nA + 15) / 16);
@@ -803,9 +804,14 @@ __global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
         const double w = a.omega[iw];
         const double fL = fermi_d(w, a.V, a.mu, a.beta), fR = fermi_d(w, 0.0, a.mu, a.beta);
         const zc *SL2 = a.SigL ? a.SigL + (size_t)iw * nfull : nullptr;
-        // SL = i (fL GamL_s + fR GamR_s) / hbar  (+ Sigma2^<)   (src/scf.f90:333-336); the
-        // loads of 8 elements a thread are issued before their stores
-        for (int base = threadIdx.x; base < nfull; base += 8 * blockDim.x) {
+        // SL = i (fL GamL_s + fR GamR_s) / hbar + Sigma2^<   (src/scf.f90:333-336). With
+        // few contact states (the usual case) the first product takes Sigma2^< itself as
+        // its B operand and the lead term is added to the contact columns of T afterwards
+        // (a rank-nc correction); otherwise SL is built in the block's scratch (the loads
+        // of 8 elements a thread issued before their stores).
+        const bool lowrank = SL2 && a.nc >= 0 && a.nc <= KD_NCMAX;
+        const zc *Bop = lowrank ? SL2 : S;
+        for (int base = threadIdx.x; !lowrank && base < nfull; base += 8 * blockDim.x) {
             zc gl[8], gr[8], s2[8];
 #pragma unroll
             for (int u = 0; u < 8; u++) {
@@ -828,7 +834,7 @@ __global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
             if (64 * hh >= nA) break;
             double cr[2][4][4], ci[2][4][4];
             const int m0 = 32 * (warp & 3), n0 = 64 * hh + 32 * (warp >> 2);
-            kd_gemm<4>(G, S, nA, 64 * hh, 64 * hh + 64, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
+            kd_gemm<4>(G, Bop, nA, 64 * hh, 64 * hh + 64, m0, n0, m0 < nA && n0 < nA, sm, cr, ci);
 #pragma unroll
             for (int mi = 0; mi < 2; mi++)
 #pragma unroll
@@ -841,6 +847,22 @@ __global__ void __launch_bounds__(256, 1) keldysh_tc(KeldyshArgs a) {
         }
         __threadfence_block();
         __syncthreads();
+        if (lowrank && a.nc > 0) {
+            // T(r, b) += sum over contact states c of G(r, c) i (fL GamL_s + fR GamR_s)(c, b), b a contact state
+            for (int t = threadIdx.x; t < nA * a.nc; t += blockDim.x) {
+                const int r = t % nA, b = a.cidx[t / nA];
+                zc acc = T[r + (size_t)b * nA];
+                for (int q = 0; q < a.nc; q++) {
+                    const int c = a.cidx[q];
+                    const size_t cb = c + (size_t)b * nA;
+                    const zc gl = a.GamLs[cb], gr = a.GamRs[cb];
+                    cfma(acc, G[r + (size_t)c * nA], zc{-(fL * gl.y + fR * gr.y), fL * gl.x + fR * gr.x});
+                }
+                T[r + (size_t)b * nA] = acc;
+            }
+            __threadfence_block();
+            __syncthreads();
+        }
         double *blk = a.out + (size_t)iw * a.nblk;
         const double *xb = a.xsub ? a.xsub + (size_t)iw * a.nblk : nullptr;
         auto put = [&](int r, int c, double vr, double vi) {
@@ -1252,6 +1274,8 @@ int sweep(qs_handle *h, int mode, double V, bool use_sigma, double *d_out, const
         k.gLd = h->d_gLd;
         k.Tws = h->d_T;
         k.err = h->d_info + 1;
+        k.cidx = h->d_kd_cidx;
+        k.nc = (h->nS == nA) ? h->kd_nc : -1;
         const int nb = (int)std::min<size_t>(h->T_slots, (size_t)n);
         const int nbt = std::min(n, 148);
         auto launch_k = [&](int v) -> int {
