@@ -949,10 +949,10 @@ def main():
         }
         if mix is not None and f64 is not None:
             line["mixed"] = {
-                "form": ("Sigma2 FFTs, 2x2 algebra and spectra in FP32, and the Keldysh products on the fastest of "
-                         "the 3xTF32 tensor-core kernel and the FP64 ones (autotuned), while max|F| is above "
-                         "max(1e-5, 100 tolf) and still falling; then FP64 steps until an FP64 residual meets tolf; "
-                         "Dyson, Broyden and observables FP64"),
+                "form": ("on fresh starts: Sigma2 FFTs, 2x2 algebra and spectra in FP32, and the Keldysh products on "
+                         "the fastest of the 3xTF32 tensor-core kernel and the FP64 ones (autotuned), while max|F| is "
+                         "above max(1e-5, 100 tolf) and still falling; then FP64 steps until an FP64 residual meets "
+                         "tolf; continued starts FP64 throughout; Dyson, Broyden and observables FP64"),
                 "value": mix["value"], "e2e": mix["e2e"], "ms_per_step": 1000.0 * mix["dev_s"] / args.steps,
                 "converged": [bool(p["converged"]) for p in mix["points"]],
                 "scf_steps_per_point": [p["n_iter"] for p in mix["points"]],

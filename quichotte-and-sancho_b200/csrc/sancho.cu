@@ -16,12 +16,13 @@
 //                         phi(q)   = sum_k1 A(k1) B(q - k1)   particle-particle bubbles
 //                         S_ph(w)  = sum_k  A(k) chi(w - k)   convolution with G_ij
 //                         S_pp(w)  = sum_k  A(k) phi(w + k)   convolution with G_ji
-//                       a block owns 128 consecutive outputs of one element and walks the
-//                       summation index in tiles: 128 values of each A sequence and the
-//                       255-long window of each B sequence the tile's outputs touch are
-//                       staged in shared memory (zero outside the sequences, so no bounds
-//                       test in the inner loop), every thread then runs the tile's
-//                       multiply-adds from shared memory (A broadcast, B consecutive)
+//                       a block of 128 threads owns 256 consecutive outputs of one element
+//                       (two adjacent ones a thread) and walks the summation index in tiles:
+//                       128 values of each A sequence and the 383-long window of each B
+//                       sequence the tile's outputs touch are staged in shared memory (zero
+//                       outside the sequences, so no bounds test in the inner loop); every
+//                       thread then runs the tile's multiply-adds from shared memory (A
+//                       broadcast, one new B value per step for its two outputs)
 //   D, E products       order 3: the U_k-weighted products of bubbles over the internal
 //                       site k at every m and q (small Na x Na products per energy)
 //   Dyson               W(w) = hbar w - H + i(GammaL + GammaR)/2 - Sigma^r(w), inverted by
