@@ -144,7 +144,7 @@ SAMPLE_N = 1024
 # timed points); 300 marks a voltage that did not converge. The CPU arm multiplies
 # its measured time per iteration by this work (the oracle runs the same algorithm, so the same
 # iterations).
-SWEEP_ITERS_B200 = dict(zip(VOLTS, [32, 27, 27, 26, 25, 25, 24, 23, 22, 21, 20, 19, 18, 16, 19, 19, 24, 24, 183, 300,
+SWEEP_ITERS_B200 = dict(zip(VOLTS, [32, 27, 27, 26, 25, 25, 24, 23, 22, 21, 20, 19, 18, 16, 17, 19, 23, 24, 110, 245,
                                     300, 300, 300, 300, 300, 300, 210, 16, 18, 20, 23, 25, 26, 27, 28, 27, 28, 29,
                                     30, 30, 31]))
 
