@@ -747,10 +747,13 @@ def setup_scan(qb):
             Sx2, Sm2 = np.kron(S, np.eye(2)), np.kron(W @ W.T, np.eye(2))
             Hn = Sm2 @ (np.kron(H0, np.eye(2)) + 0.5 * (Sx2 @ Lam + Lam @ Sx2)) @ Sm2
             return 0.5 * (Hn + Hn.conj().T)
-        rep = 3 if N <= 256 else 1
-        (H, _), tg = wall(lambda: qb.dftb_lowdin(S, H0, Lam, True), rep)
+        rep = 3
+        calls = []
+        for _ in range(rep):  # each call timed: the spread between calls of one size
+            (H, _), t1 = wall(lambda: qb.dftb_lowdin(S, H0, Lam, True), 1)
+            calls.append(t1)
         Hn, tc = wall(ref, rep)
-        out[f"lowdin_N{N}"] = {"device_s": tg, "numpy_s": tc,
+        out[f"lowdin_N{N}"] = {"device_s": min(calls), "device_calls_s": calls, "numpy_s": tc,
                                "rel_err": float(np.max(np.abs(H - Hn)) / np.max(np.abs(Hn)))}
     return {"setup_scan": out, "numpy_threads": os.cpu_count()}
 

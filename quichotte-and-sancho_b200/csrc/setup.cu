@@ -27,12 +27,45 @@
 // first scaled by an exact power of two (jac_scale), so the sums of squares stay in range.
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "qs_common.cuh"
 
 namespace qs {
 namespace {
+
+// Work buffers of the set-up come from a memory pool of their own per device that keeps up
+// to 4 GiB of freed memory mapped between calls (the default pool returns it at every
+// synchronisation, so each call of a large size mapped its buffers again, at a cost that
+// varied from call to call). It stays apart from the default pool that the solver handles use,
+// whose free memory the serving loop's admission reads.
+cudaError_t setup_alloc(void **p, size_t bytes, cudaStream_t st) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = pools.find(dev);
+        if (it == pools.end()) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+            uint64_t keep = 4ull << 30;
+            if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+            pools[dev] = pool;
+        } else {
+            pool = it->second;
+        }
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
 
 constexpr int JAC_MAX_N = 2048;
 constexpr int JAC_MAX_SWEEPS = 60;
@@ -317,12 +350,12 @@ cudaError_t eigh_dev(cudaStream_t st, int N, int batch, zc *dA, double *dE, int 
     do {                                    \
         if ((e = (x)) != cudaSuccess) goto out; \
     } while (0)
-    JAC_TRY(cudaMallocAsync(&dflag, sizeof(int) * (2 * batch + 1), st));
+    JAC_TRY(setup_alloc((void **)&dflag, sizeof(int) * (2 * batch + 1), st));
     dact = dflag + batch;
     dexpo = dact + 1;
-    JAC_TRY(cudaMallocAsync(&drank, sizeof(int) * (size_t)N * batch, st));
-    JAC_TRY(cudaMallocAsync(&dpairs, sizeof(JacPair) * (size_t)S * batch, st));
-    JAC_TRY(cudaMallocAsync(&drows, sizeof(JacRow) * (size_t)M * batch, st));
+    JAC_TRY(setup_alloc((void **)&drank, sizeof(int) * (size_t)N * batch, st));
+    JAC_TRY(setup_alloc((void **)&dpairs, sizeof(JacPair) * (size_t)S * batch, st));
+    JAC_TRY(setup_alloc((void **)&drows, sizeof(JacRow) * (size_t)M * batch, st));
     JAC_TRY(smem_cap((const void *)jac_rotate));
     JAC_TRY(smem_cap((const void *)jac_sort));
     JAC_TRY(cudaMemsetAsync(dflag, 0, sizeof(int) * (batch + 1), st));
@@ -733,10 +766,10 @@ int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, 
     std::vector<int> hinfo(batch, 0);
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return -(int)e;
-    if ((e = cudaMallocAsync(&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
-        (e = cudaMallocAsync(&dW, sizeof(zc) * nn, st)) == cudaSuccess &&
-        (e = cudaMallocAsync(&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
-        (e = cudaMallocAsync(&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
+    if ((e = setup_alloc((void **)&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (e = setup_alloc((void **)&dW, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (e = setup_alloc((void **)&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
+        (e = setup_alloc((void **)&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
         (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess &&
         (e = eigh_dev(st, N, batch, dA, dE, dinfo, dW)) == cudaSuccess &&
         (e = cudaMemcpyAsync(A, dA, sizeof(zc) * nn, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
@@ -772,10 +805,10 @@ int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return -(int)e;
     const bool small = N <= JV_MAX_N;
-    if ((e = cudaMallocAsync(&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
-        (small || (e = cudaMallocAsync(&dW, sizeof(zc) * nn, st)) == cudaSuccess) &&
-        (e = cudaMallocAsync(&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
-        (e = cudaMallocAsync(&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
+    if ((e = setup_alloc((void **)&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
+        (small || (e = setup_alloc((void **)&dW, sizeof(zc) * nn, st)) == cudaSuccess) &&
+        (e = setup_alloc((void **)&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
+        (e = setup_alloc((void **)&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
         (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess) {
         if (small) {
             if ((e = smem_cap((const void *)jac_values)) == cudaSuccess) {
@@ -828,9 +861,9 @@ int qs_dftb_lowdin(int N, const double *S, const double *H0, const double *Lam, 
     } while (0)
     // n1 blocks: S then its eigenvectors, the eigensolver's workspace, S^-1/2;
     // n2 blocks: Sm2, Lam, Hao, T, Hn.  dR: S, H0 (real), the eigenvalues of S
-    LOW_TRY(cudaMallocAsync(&buf, sizeof(zc) * (3 * n1 + 5 * n2), st));
-    LOW_TRY(cudaMallocAsync(&dR, sizeof(double) * (2 * n1 + N), st));
-    LOW_TRY(cudaMallocAsync(&dinfo, sizeof(int), st));
+    LOW_TRY(setup_alloc((void **)&buf, sizeof(zc) * (3 * n1 + 5 * n2), st));
+    LOW_TRY(setup_alloc((void **)&dR, sizeof(double) * (2 * n1 + N), st));
+    LOW_TRY(setup_alloc((void **)&dinfo, sizeof(int), st));
     {
         zc *dS = buf, *dW = buf + n1, *dSmh = buf + 2 * n1;
         zc *dSm2 = buf + 3 * n1, *dLam = dSm2 + n2, *dHao = dLam + n2, *dT = dHao + n2, *dHn = dT + n2;
