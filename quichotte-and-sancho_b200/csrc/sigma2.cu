@@ -405,16 +405,18 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Kernel A: tile = 4 adjacent sequences x GA adjacent m2 (GA = 4: one block of 16 warps per
-// SM; GA = 2: two blocks of 8 warps, whose phases interleave); tiles ordered sequence-tile
-// fastest. The FP64 values are copied into a staging buffer; with T = float they are
-// converted into a work buffer before the transforms (Y then holds FP32 spectra).
-template <typename T, int N1, int GA>
-__global__ void __launch_bounds__(128 * GA, 4 / GA) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk, int n,
-                                                              const int2 *__restrict__ desc, int nY, FftPlan fp,
-                                                              const zc *__restrict__ tw, cplx<T> *__restrict__ Y,
-                                                              int nitems) {
-    constexpr int SA = 4, NS = SA * GA;  // one warp per sequence: blockDim.x = 32 NS
+// Kernel A: tile = SA adjacent sequences x GA adjacent m2 (SA = 4, GA = 4: one block of 16
+// warps per SM; SA = 4, GA = 2: two blocks of 8 warps, whose phases interleave; SA = 2,
+// GA = 8: one block of 16 warps whose Y rows are written in 128-byte runs, FP64 only);
+// tiles ordered sequence-tile fastest. The FP64 values are copied into a staging buffer;
+// with T = float they are converted into a work buffer before the transforms (Y then holds
+// FP32 spectra).
+template <typename T, int N1, int GA, int SA = 4>
+__global__ void __launch_bounds__(32 * SA * GA, 16 / (SA * GA)) sig2_fwdA_p(const double *__restrict__ X, int64_t nblk,
+                                                                        int n, const int2 *__restrict__ desc, int nY,
+                                                                        FftPlan fp, const zc *__restrict__ tw,
+                                                                        cplx<T> *__restrict__ Y, int nitems) {
+    constexpr int NS = SA * GA;  // one warp per sequence: blockDim.x = 32 NS
     constexpr bool F64 = sizeof(T) == 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
@@ -620,6 +622,15 @@ using InvCPFn = void (*)(const cplx<T> *, zc *, zc *, int, int, int, const doubl
 // persistent kernels A / C for power-of-two N1; w = 4 (16-sequence tiles, one block per
 // SM) or 2 (8-sequence tiles, two blocks per SM)
 template <typename T> static FwdAPFn<T> pick_fwdA_p(int N1, int w) {
+    if (w == 8) {  // two sequences x eight m2 (FP64: the twiddle columns of 8 m2 fit next to the staging)
+        if (sizeof(T) != 8) return nullptr;
+        switch (N1) {
+            case 64: return sig2_fwdA_p<T, 64, 8, 2>;
+            case 128: return sig2_fwdA_p<T, 128, 8, 2>;
+            case 256: return sig2_fwdA_p<T, 256, 8, 2>;
+        }
+        return nullptr;
+    }
     if (w == 2) switch (N1) {
             case 64: return sig2_fwdA_p<T, 64, 2>;
             case 128: return sig2_fwdA_p<T, 128, 2>;
@@ -645,8 +656,10 @@ template <typename T> static InvCPFn<T> pick_invC_p(int N1, int w) {
     }
     return nullptr;
 }
+// kernel A's tile: w adjacent m2 x (w == 8 ? 2 : 4) adjacent sequences
+static int fwdA_sa(int w) { return w == 8 ? 2 : 4; }
 template <typename T> static size_t smem_fwdA_p(int N1, int w) {
-    const size_t PL = padded_len(N1), ns = 4 * w;
+    const size_t PL = padded_len(N1), ns = (size_t)fwdA_sa(w) * w;
     return sizeof(zc) * (2 * ns * PL + 2 * (size_t)w * N1) + (sizeof(T) == 8 ? 0 : sizeof(cplx<T>) * ns * PL) +
            sizeof(cplx<T>) * fft_table_len(N1);
 }
@@ -676,6 +689,7 @@ template <typename T> static int sigma2_attributes(qs_handle *h) {
             QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1, w)));
             QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1, w)));
         }
+    if (persistent_AC(fp) && pick_fwdA_p<T>(fp.N1, 8)) QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1, 8)));
     return 0;
 }
 
@@ -780,10 +794,17 @@ template <typename T> static int sigma2_run(qs_handle *h, const double *d_x) {
     const int cand[2] = {4, 2};  // tile widths, autotuned per size (results are identical)
     const int key = tune_key(nA, h->n) + (sizeof(T) == 4 ? 1 << 20 : 0);
     if (pers) {
-        int rc = tune_launch(h, TUNE_SIG2_A, key, cand, 2, 4, [&](int w) -> int {
-            const int nitems = (int)((h->nY + 3) / 4) * (fp.N2 / w);
+        // kernel A: the FP64 form also has the 2 x 8 tile (128-byte Y runs)
+        const int candA[3] = {4, 2, 8};
+        const bool wide = sizeof(T) == 8 && fp.N2 % 8 == 0 &&
+                          smem_fwdA_p<T>(fp.N1, 8) + 2048 <= (size_t)SMEM_MAX;
+        int rc = tune_launch(h, TUNE_SIG2_A, key, candA, wide ? 3 : 2, 4, [&](int w) -> int {
+            const int sa = fwdA_sa(w);
+            const int nitems = (int)((h->nY + sa - 1) / sa) * (fp.N2 / w);
+            const int per_sm = 16 / (sa * w);
+            const auto fn = pick_fwdA_p<T>(fp.N1, w);
             int pa = prof_begin(h, K_SIG2A);
-            pick_fwdA_p<T>(fp.N1, w)<<<std::min(nitems, 148 * (4 / w)), 128 * w, smem_fwdA_p<T>(fp.N1, w), h->stream>>>(
+            fn<<<std::min(nitems, 148 * per_sm), 32 * sa * w, smem_fwdA_p<T>(fp.N1, w), h->stream>>>(
                 d_x, h->nblk, h->n, h->d_ydesc, (int)h->nY, fp, h->d_tw, Y, nitems);
             prof_end(h, pa);
             QS_CUDA(h, cudaGetLastError());
