@@ -559,6 +559,82 @@ __global__ void __launch_bounds__(128 * GC, 4 / GC) sig2_invC_p(const cplx<T> *_
     }
 }
 
+// Kernel C with a tile of two site pairs (I, I+1) of one output column (J, bb): the 16
+// sequences are Sigma^R and Sigma^< of rows 2I .. 2I+3 x 2 adjacent m2, so each energy's four
+// rows go out as one 64-byte run (V is read in 32-byte runs). One block of 16 warps per SM.
+template <typename T, int N1>
+__global__ void __launch_bounds__(512, 1) sig2_invC_p2(const cplx<T> *__restrict__ V, zc *__restrict__ SigR,
+                                                       zc *__restrict__ SigL, int nA, int nAs, int n,
+                                                       const double *__restrict__ Upair, FftPlan fp,
+                                                       const zc *__restrict__ tw, int nitems) {
+    constexpr int GC = 2, NR = 4, NS = 2 * NR * GC;  // stage x row x m2
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N2 = fp.N2, Nf = fp.Nf, PL = padded_len(N1);
+    const int nmt = N2 / GC, nfull = nA * nA, nI2 = (nAs + 1) / 2;
+    const int m1max = (n + N2 - 1) / N2;
+    cplx<T> *buf0 = (cplx<T> *)smem_raw;
+    cplx<T> *twL = buf0 + 2 * NS * PL;
+    fft_table_fill(twL, N1, tw, N2);
+    // item -> output column, first row, m2 block, the two pairs' scales (0: no interaction
+    // or no second pair)
+    auto tile = [&](int it, int &io, int &jo, int &bb, int &m20, double &c0, double &c1) {
+        const int pc = it / nmt;
+        m20 = (it % nmt) * GC;
+        bb = pc & 1;
+        const int q = pc >> 1, I = 2 * (q % nI2), J = q / nI2;
+        io = 2 * I;
+        jo = 2 * J;
+        c0 = Upair[I + J * nAs];
+        c1 = (I + 1 < nAs) ? Upair[I + 1 + J * nAs] : 0.0;
+    };
+    auto load = [&](int it, cplx<T> *b) {
+        int io, jo, bb, m20;
+        double c0, c1;
+        tile(it, io, jo, bb, m20, c0, c1);
+        for (int t = threadIdx.x; t < NS * N1; t += blockDim.x) {
+            const int gl = t % GC, r = t / GC, sl = r % (2 * NR), l1 = r / (2 * NR);
+            const int a = sl % NR, st = sl / NR;
+            if ((a < 2 ? c0 : c1) == 0.0) continue;  // a zero block: nothing to read
+            const size_t sid = (size_t)st * nfull + (io + a) + (size_t)(jo + bb) * nA;
+            cp_async_elem(b + (sl * GC + gl) * PL + pidx(l1), V + sid * Nf + (size_t)l1 * N2 + m20 + gl, true);
+        }
+    };
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, G = fft_group(N1);
+    if (blockIdx.x < nitems) load(blockIdx.x, buf0);
+    cp_async_commit();
+    int cur = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int nxt = it + gridDim.x;
+        if (nxt < nitems) load(nxt, buf0 + (cur ^ 1) * NS * PL);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        int io, jo, bb, m20;
+        double c0, c1;
+        tile(it, io, jo, bb, m20, c0, c1);
+        cplx<T> *b = buf0 + cur * NS * PL;
+        for (int q = warp * G; q < NS; q += nw * G) {
+            // sequence q = (st NR + a) GC + gl; skip the transforms of zero blocks
+            const int a = (q / GC) % NR;
+            if ((a < 2 ? c0 : c1) != 0.0) warp_fft_pow2<T, N1>(b + q * PL, PL, min(G, NS - q), +1, twL);
+        }
+        __syncthreads();
+        // lanes: row a fastest (64-byte global runs), then m2, then stage
+        for (int t = threadIdx.x; t < NS * m1max; t += blockDim.x) {
+            const int a = t % NR, gl = (t / NR) % GC, st = (t / (NR * GC)) & 1, m1 = t / NS;
+            const int64_t w = (int64_t)N2 * m1 + m20 + gl;
+            const double c = a < 2 ? c0 : c1;
+            if (w < n && (a < 2 || io + a < nA)) {
+                cplx<T> v = (c != 0.0) ? b[((st * NR + a) * GC + gl) * PL + pidx(m1)] : cplx<T>{0, 0};
+                zc *S = st ? SigL : SigR;
+                S[w * nfull + (io + a) + (size_t)(jo + bb) * nA] = zc{c * (double)v.x, c * (double)v.y};
+            }
+        }
+        __syncthreads();  // the buffer is rewritten by the next tiles
+        cur ^= 1;
+    }
+}
+
 // ---------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------
@@ -644,6 +720,15 @@ template <typename T> static FwdAPFn<T> pick_fwdA_p(int N1, int w) {
     return nullptr;
 }
 template <typename T> static InvCPFn<T> pick_invC_p(int N1, int w) {
+    if (w == 8) {  // two site pairs x two m2 (FP64)
+        if (sizeof(T) != 8) return nullptr;
+        switch (N1) {
+            case 64: return sig2_invC_p2<T, 64>;
+            case 128: return sig2_invC_p2<T, 128>;
+            case 256: return sig2_invC_p2<T, 256>;
+        }
+        return nullptr;
+    }
     if (w == 2) switch (N1) {
             case 64: return sig2_invC_p<T, 64, 2>;
             case 128: return sig2_invC_p<T, 128, 2>;
@@ -664,7 +749,8 @@ template <typename T> static size_t smem_fwdA_p(int N1, int w) {
            sizeof(cplx<T>) * fft_table_len(N1);
 }
 template <typename T> static size_t smem_invC_p(int N1, int w) {
-    return sizeof(cplx<T>) * ((size_t)2 * 4 * w * padded_len(N1) + (size_t)fft_table_len(N1));
+    const size_t ns = (w == 8) ? 16 : (size_t)4 * w;
+    return sizeof(cplx<T>) * ((size_t)2 * ns * padded_len(N1) + (size_t)fft_table_len(N1));
 }
 template <typename T> static size_t smem_A(const qs_handle *h) {
     return sizeof(cplx<T>) * ((size_t)(h->sig2_SA * h->sig2_GA + 8) * padded_len(h->fft.N1) + fft_table_len(h->fft.N1));
@@ -690,6 +776,7 @@ template <typename T> static int sigma2_attributes(qs_handle *h) {
             QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1, w)));
         }
     if (persistent_AC(fp) && pick_fwdA_p<T>(fp.N1, 8)) QS_CUDA(h, smem_cap((const void *)pick_fwdA_p<T>(fp.N1, 8)));
+    if (persistent_AC(fp) && pick_invC_p<T>(fp.N1, 8)) QS_CUDA(h, smem_cap((const void *)pick_invC_p<T>(fp.N1, 8)));
     return 0;
 }
 
@@ -828,10 +915,15 @@ template <typename T> static int sigma2_run(qs_handle *h, const double *d_x) {
         QS_CUDA(h, cudaGetLastError());
     }
     if (pers) {
-        int rc = tune_launch(h, TUNE_SIG2_C, key, cand, 2, 4, [&](int w) -> int {
-            const int nitems = 2 * h->nAs * h->nAs * (fp.N2 / w);
+        // kernel C: the FP64 form also has the two-site-pair tile (64-byte Sigma runs)
+        const int candC[3] = {4, 2, 8};
+        const bool wide = sizeof(T) == 8 && fp.N2 % 2 == 0;
+        int rc = tune_launch(h, TUNE_SIG2_C, key, candC, wide ? 3 : 2, 4, [&](int w) -> int {
+            const int nitems = (w == 8) ? 2 * ((h->nAs + 1) / 2) * h->nAs * (fp.N2 / 2)
+                                        : 2 * h->nAs * h->nAs * (fp.N2 / w);
+            const int thr = (w == 8) ? 512 : 128 * w, per_sm = (w == 8) ? 1 : 4 / w;
             int pc = prof_begin(h, K_SIG2C);
-            pick_invC_p<T>(fp.N1, w)<<<std::min(nitems, 148 * (4 / w)), 128 * w, smem_invC_p<T>(fp.N1, w), h->stream>>>(
+            pick_invC_p<T>(fp.N1, w)<<<std::min(nitems, 148 * per_sm), thr, smem_invC_p<T>(fp.N1, w), h->stream>>>(
                 V, h->d_SigR, h->d_SigL, nA, h->nAs, h->n, h->sig2_Upair, fp, h->d_tw, nitems);
             prof_end(h, pc);
             QS_CUDA(h, cudaGetLastError());
