@@ -171,10 +171,12 @@ def test_sigma2_and_residual_match_oracle_over_fft_lengths(delta):
 POW2_DELTAS = [0.0037309, 0.0018609, 0.0009293, 0.0004655]
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
 @pytest.mark.parametrize("delta", POW2_DELTAS)
 def test_sigma2_power_of_two_fft_lengths_match_oracle(delta, mode):
-    """mode 1: autotuned; 2 / 3: the 16- / 8-sequence tiles of the persistent kernels A, C"""
+    """mode 1: autotuned; 2: the 4 x 4 tiles of the persistent kernels A and C; 3: the FP64
+    forms' wide tiles (A: 2 sequences x 8 columns, C: two site pairs x 2 columns); 4: the
+    4 x 2 tiles (two blocks per SM)"""
     m = small_helix(delta)
     qb.autotune(mode)
     try:
