@@ -4,8 +4,9 @@
 //                             zheev) over a batch of matrices of one size.
 //   qs_hermitian_eigenvalues  the same without eigenvectors (zheev JOBZ = 'N'), which is all
 //                             the energy grid needs (src/quichotte.f90:79-83): for N <= 160
-//                             one block per matrix with the matrix in shared memory
-//                             (jac_values below).
+//                             one block per matrix with the matrix in shared memory,
+//                             Householder tridiagonalisation and Sturm multisection
+//                             (tri_values below).
 //   qs_dftb_lowdin            the dense part of build_hamiltonian_from_dftb_hs
 //                             (src/hamiltonian.f90:625-640, 680-689): S^-1/2 from the
 //                             eigenpairs of S (dsyev there), the SOC form on the spin-doubled
@@ -419,218 +420,335 @@ out:
 }
 
 // ---- eigenvalues only: one block per matrix, the matrix in shared memory ----
-// The upper triangle is packed by columns, (i, j) with i <= j at i + j (j + 1) / 2, so a matrix
-// of order N <= 160 fits one block's shared memory. One rotation round maps every 2x2 block
-// B = A[{p, q}, {p', q'}] of two pairs to J_P^H B J_P' (a pair's own diagonal block becomes
-// diag(app', aqq')); each block is read and written by one thread, so a round needs no second
-// buffer and every sweep runs inside one launch, with block barriers between the phases.
-constexpr int JV_MAX_N = 160, JV_THREADS = 512;
+// Two phases, both inside one launch:
+//  1. Householder reduction to a real tridiagonal matrix, with zhetd2's reflectors
+//     H = I - tau v v^H (v(1) = 1, beta real, tau and v as zlarfg forms them) applied as
+//     A22 <- A22 - v w^H - w v^H, w = p - (tau/2)(p^H v) v, p = tau A22 v. The lower triangle
+//     is packed by columns, (i, j) with i >= j at col(j) + i - j, so N <= 160 fits one
+//     block's shared memory; the trailing matrix-vector product runs as G x m thread
+//     partials (no atomics, a fixed summation order), the rank-2 update one warp per column,
+//     and warp 0 forms the next reflector as soon as its column is updated (four block
+//     barriers per column). Shared-memory bandwidth bounds this phase: every step reads the
+//     trailing matrix twice (Hermitian, one triangle stored) and updates it once.
+//  2. The eigenvalues of the tridiagonal matrix (d, e^2) by Sturm counts (tv_count): one count
+//     per thread at 512 points of the Gershgorin interval brackets every eigenvalue, then
+//     G threads per eigenvalue split its bracket into G + 1 parts per step until the bracket
+//     is 2 eps ||T|| wide. A diagonal entry isolated by zero couplings is an eigenvalue as it
+//     stands and is returned exactly (a diagonal matrix gives its own entries).
+// Results are deterministic: every sum has a fixed order.
+constexpr int TV_MAX_N = 160, TV_THREADS = 512, TV_WARPS = TV_THREADS / 32;
 
-__device__ __forceinline__ int pk(int i, int j) { return i + j * (j + 1) / 2; }  // i <= j
-__device__ __forceinline__ zc pget(const zc *P, int a, int b) { return a <= b ? P[pk(a, b)] : conj(P[pk(b, a)]); }
-__device__ __forceinline__ void pset(zc *P, int a, int b, zc v) {
-    if (a <= b) P[pk(a, b)] = v;
-    else P[pk(b, a)] = conj(v);
+__device__ __forceinline__ int tv_col(int j, int N) { return j * N - j * (j - 1) / 2; }
+
+// The number of eigenvalues of the tridiagonal (d, e2) below the shift s: the sign changes of
+// the leading principal minors of T - s, p_0 = d_0 - s, p_i = (d_i - s) p_{i-1} - e_{i-1}^2 p_{i-2}
+// (p_{-1} = 1), that is the negative pivots q_i = p_i / p_{i-1} of T - s = L D L^T, without a
+// division per step. A minor that vanishes (exactly, or by underflow) is replaced by
+// -2^-100 p_{i-1}, a negative pivot, as dstebz replaces a pivot |q| <= pivmin by -pivmin; the
+// sign tests read the sign bits (integer operations). After every fourth step the pair
+// (p_i, p_{i-1}) is rescaled by a power of two into 2^-300 .. 2^300 (exact, signs unchanged);
+// with the matrix scaled to entries below 2, four steps stay far inside the double range. Per
+// step this is one FMA on the dependence chain instead of a division (measured on B200: ~120
+// cycles per step with 15 warps counting, against ~226 for the division form).
+__device__ __forceinline__ int tv_count(const double *d, const double *e2, int N, double s) {
+    double pc = d[0] - s, pm = 1.0;
+    if (pc == 0.0) pc = -0x1p-100;
+    int c = (int)((unsigned long long)__double_as_longlong(pc) >> 63);
+    auto step = [&](double di, double ei) {
+        double pn = fma(di - s, pc, -ei * pm);
+        const double tiny = -0x1p-100 * pc;  // off the dependence chain
+        if (pn == 0.0) pn = tiny;
+        c += (int)((unsigned long long)(__double_as_longlong(pn) ^ __double_as_longlong(pc)) >> 63);
+        pm = pc;
+        pc = pn;
+    };
+    int i = 1;
+    for (; i + 3 < N; i += 4) {
+        const double d0 = d[i], d1 = d[i + 1], d2 = d[i + 2], d3 = d[i + 3];
+        const double e0 = e2[i - 1], e1 = e2[i], f2 = e2[i + 1], f3 = e2[i + 2];
+        step(d0, e0);
+        step(d1, e1);
+        step(d2, f2);
+        step(d3, f3);
+        const double mx = fmax(fabs(pc), fabs(pm));
+        const double f = mx > 0x1p300 ? 0x1p-300 : (mx < 0x1p-300 ? 0x1p300 : 1.0);
+        pc *= f;
+        pm *= f;
+    }
+    for (; i < N; i++) step(d[i], e2[i - 1]);
+    return c;
 }
 
-constexpr int JV_TASKS = 8;  // 2x2 blocks per thread: S (S + 1) / 2 <= 3240 <= 8 x 512
-
-inline size_t jv_smem(int N) {
-    const size_t M = N + (N & 1), S = M / 2, np = (size_t)N * (N + 1) / 2;
-    return 16 * np + 48 * S + 8 * S + 8 * (size_t)N;
+inline size_t tv_smem(int N) {
+    return sizeof(zc) * ((size_t)N * (N + 1) / 2 + 3 * (size_t)N + TV_THREADS) + sizeof(double) * 3 * (size_t)N;
 }
 
-__global__ void __launch_bounds__(JV_THREADS) jac_values(int N, const zc *__restrict__ A, double *__restrict__ E,
+// reflector k (zlarfg on column k below the diagonal), by one warp: d_k, e_k^2, tau and scale, and
+// v = (1, x / (alpha - beta)) into vk; tau = 0 when there is nothing to annihilate (H = I)
+__device__ __forceinline__ void tv_reflector(const zc *L, int N, int k, double *d, double *e2, zc *tau_s, zc *vk) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, m = N - k - 1;
+    const zc *col = L + tv_col(k, N);  // col[0] = L(k, k), col[1 + i] = L(k + 1 + i, k)
+    double xn = 0.0;
+    for (int i = 1 + lane; i < m; i += 32) xn += col[1 + i].x * col[1 + i].x + col[1 + i].y * col[1 + i].y;
+    for (int o = 16; o; o >>= 1) xn += __shfl_xor_sync(FULL, xn, o);
+    xn = __shfl_sync(FULL, xn, 0);  // one value for every lane
+    const zc al = col[1];
+    zc t{0.0, 0.0}, sc{0.0, 0.0};
+    double ee = al.x * al.x + al.y * al.y;
+    if (!(m == 1 || (xn == 0.0 && al.y == 0.0))) {
+        const double beta = -copysign(sqrt(ee + xn), al.x);
+        const double zx = al.x - beta, zz = zx * zx + al.y * al.y;  // |alpha - beta|^2 >= beta^2 > 0
+        const double rb = 1.0 / beta, rz = 1.0 / zz;
+        t = zc{(beta - al.x) * rb, -al.y * rb};
+        sc = zc{zx * rz, -al.y * rz};  // 1 / (alpha - beta)
+        ee = beta * beta;
+        for (int i = lane; i < m; i += 32) vk[i] = (i == 0) ? zc{1.0, 0.0} : col[1 + i] * sc;
+    }
+    if (lane == 0) {
+        d[k] = col[0].x;
+        e2[k] = ee;
+        *tau_s = t;
+    }
+}
+
+__global__ void __launch_bounds__(TV_THREADS, 1) tri_values(int N, const zc *__restrict__ A, double *__restrict__ E,
                                                         int *__restrict__ info) {
-    extern __shared__ __align__(16) unsigned char jv_raw[];
-    const int M = N + (N & 1), S = M / 2, np = N * (N + 1) / 2, nblk = S * (S + 1) / 2;
-    zc *P = (zc *)jv_raw;               // packed upper triangle
-    zc *pph = P + np;                   // per pair: the phase of A(p, q)
-    double *pc = (double *)(pph + S);   // c
-    double *ps = pc + S;                // s
-    double *pa = ps + S;                // app after the rotation
-    double *pb = pa + S;                // aqq after the rotation
-    int *sp = (int *)(pb + S);          // the pair of each slot in this round: p
-    int *sq = sp + S;                   //                                      q
-    double *dk = (double *)(sq + S);    // the eigenvalues, for the sort
-    __shared__ double red_off[JV_THREADS / 32], red_tot[JV_THREADS / 32];
-    __shared__ int go, ex_s;
-    const int b = blockIdx.x, tid = threadIdx.x;
-    // this thread's 2x2 blocks (P1 <= P2 over the slots), the same in every round
-    int task[JV_TASKS];
-    int ntask = 0;
-#pragma unroll
-    for (int u = 0; u < JV_TASKS; u++) {
-        const int t = tid + u * JV_THREADS;
-        task[u] = 0;
-        if (t < nblk) {
-            int P2 = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-            while (P2 * (P2 + 1) / 2 > t) P2--;
-            while ((P2 + 1) * (P2 + 2) / 2 <= t) P2++;
-            task[u] = (P2 << 16) | (t - P2 * (P2 + 1) / 2);
-            ntask = u + 1;
-        }
-    }
+    extern __shared__ __align__(16) unsigned char tv_raw[];
+    const int np = N * (N + 1) / 2;
+    zc *L = (zc *)tv_raw;    // packed lower triangle
+    zc *v = L + np;          // the reflectors k and k + 1 (two buffers)
+    zc *w = v + 2 * N;       // w of the rank-2 update
+    zc *part = w + N;        // the matrix-vector partials; the 512 Sturm counts of the bracketing pass
+    double *d = (double *)(part + TV_THREADS), *e2 = d + N, *ev = e2 + N;
+    __shared__ double red[TV_WARPS][2];
+    __shared__ zc tau_s[2];
+    __shared__ double glo_s, ghi_s, piv_s, tol_s;
+    __shared__ int ex_s, bad_s;
+    const unsigned FULL = 0xffffffffu;
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const zc *a = A + (int64_t)b * N * N;
-    for (int e = tid; e < N * N; e += blockDim.x) {
-        const int i = e % N, j = e / N;
-        if (i < j) P[pk(i, j)] = a[e];
-        else if (i == j) P[pk(i, i)] = zc{a[e].x, 0.0};
-    }
-    __syncthreads();
-    {  // scale by 2^-ex so that the largest |Re| or |Im| lies in [1, 2) (as jac_scale)
+    // L(j, i) = conj(A(i, j)) from the upper triangle (i < j), the diagonal's real part
+    {
         double m = 0.0;
-        for (int e = tid; e < np; e += blockDim.x) m = fmax(m, fmax(fabs(P[e].x), fabs(P[e].y)));
-        for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((tid & 31) == 0) red_off[tid >> 5] = m;
-        __syncthreads();
-        if (tid == 0) {
-            m = 0.0;
-            for (int w = 0; w < JV_THREADS / 32; w++) m = fmax(m, red_off[w]);
-            ex_s = (m > 0.0 && m < INFINITY) ? ilogb(m) : 0;
-        }
-        __syncthreads();
-        const int ex = ex_s;
-        if (ex != 0)
-            for (int e = tid; e < np; e += blockDim.x) P[e] = zc{ldexp(P[e].x, -ex), ldexp(P[e].y, -ex)};
-    }
-    const double ne = (double)N * 2.220446049250313e-16;
-    for (int sweep = 0;; sweep++) {
-        __syncthreads();
-        // convergence: off-diagonal weight at rounding level (every thread reads the verdict)
-        double off = 0.0, tot = 0.0;
-        for (int e = tid; e < N * N; e += blockDim.x) {
+        int bad = 0;
+        for (int e = tid; e < N * N; e += TV_THREADS) {
             const int i = e % N, j = e / N;
             if (i > j) continue;
-            const zc v = P[pk(i, j)];
-            const double w = v.x * v.x + v.y * v.y;
-            if (i == j) tot += w;
-            else off += 2.0 * w;
+            const zc x = a[e];
+            const zc y = (i == j) ? zc{x.x, 0.0} : zc{x.x, -x.y};
+            L[tv_col(i, N) + j - i] = y;
+            bad |= !(isfinite(y.x) && isfinite(y.y));
+            m = fmax(m, fmax(fabs(y.x), fabs(y.y)));
         }
         for (int o = 16; o; o >>= 1) {
-            off += __shfl_xor_sync(0xffffffffu, off, o);
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            m = fmax(m, __shfl_xor_sync(FULL, m, o));
+            bad |= __shfl_xor_sync(FULL, bad, o);
         }
-        if ((tid & 31) == 0) {
-            red_off[tid >> 5] = off;
-            red_tot[tid >> 5] = tot;
+        if (lane == 0) {
+            red[warp][0] = m;
+            red[warp][1] = bad;
         }
         __syncthreads();
         if (tid == 0) {
-            off = 0.0;
-            tot = 0.0;
-            for (int w = 0; w < JV_THREADS / 32; w++) {
-                off += red_off[w];
-                tot += red_tot[w];
+            double mm = 0.0;
+            int bb = 0;
+            for (int q = 0; q < TV_WARPS; q++) {
+                mm = fmax(mm, red[q][0]);
+                bb |= red[q][1] != 0.0;
             }
-            tot += off;
-            int g = 1;
-            if (!(off < INFINITY) || !(tot < INFINITY)) g = -1;  // non-finite entries
-            else if (off <= ne * ne * tot) g = 0;
-            else if (sweep >= JAC_MAX_SWEEPS) g = -1;
-            go = g;
-            if (g != 1) info[b] = (g == 0) ? 0 : 1;
+            // scale by 2^-ex so that the largest |Re| or |Im| lies in [1, 2), as LAPACK scales
+            ex_s = (mm > 0.0 && mm < INFINITY) ? ilogb(mm) : 0;
+            bad_s = bb;
+            info[b] = bb;  // non-finite entries: info = 1, no eigenvalues
         }
         __syncthreads();
-        if (go != 1) break;
-        for (int r = 0; r < M - 1; r++) {
-            if (tid < S) {  // the rotation of pair tid (as jac_params)
-                int p, q;
-                jac_slot(M, r, tid, p, q);
-                double c = 1.0, s = 0.0, phx = 1.0, phy = 0.0;
-                double app = P[pk(p, p)].x, aqq = 0.0;
-                if (q < N) {
-                    aqq = P[pk(q, q)].x;
-                    const zc apq = P[pk(p, q)];
-                    const double mag = hypot(apq.x, apq.y);
-                    if (mag > 0.0) {
-                        const double tau = (aqq - app) / (2.0 * mag);
-                        const double tt =
-                            fabs(tau) > 1e150 ? 0.5 / tau : copysign(1.0, tau) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + tt * tt);
-                        s = tt * c;
-                        phx = apq.x / mag;
-                        phy = apq.y / mag;
-                        app -= tt * mag;
-                        aqq += tt * mag;
-                    }
-                }
-                pc[tid] = c;
-                ps[tid] = s;
-                pph[tid] = zc{phx, phy};
-                pa[tid] = app;
-                pb[tid] = aqq;
-                sp[tid] = p;
-                sq[tid] = q;
-            }
+        if (bad_s) {
+            for (int i = tid; i < N; i += TV_THREADS) E[(int64_t)b * N + i] = NAN;
+            return;
+        }
+        if (ex_s != 0)
+            for (int e = tid; e < np; e += TV_THREADS) L[e] = zc{ldexp(L[e].x, -ex_s), ldexp(L[e].y, -ex_s)};
+        __syncthreads();
+    }
+    // phase 1: reflector k annihilates column k below the subdiagonal. Warp 0 forms reflector
+    // k + 1 as soon as it has updated column k + 1, while the other warps finish the update of
+    // step k (v and tau alternate between two buffers).
+    if (warp == 0 && N > 1) tv_reflector(L, N, 0, d, e2, &tau_s[0], v);
+    __syncthreads();
+    for (int k = 0; k + 1 < N; k++) {
+        const int s = k + 1, m = N - s;
+        const zc t = tau_s[k & 1];
+        const zc *vk = v + (k & 1) * N;
+        zc *vn = v + ((k + 1) & 1) * N;
+        const bool next = k + 2 < N;  // reflector k + 1 exists
+        if (t.x == 0.0 && t.y == 0.0) {
+            if (warp == 0 && next) tv_reflector(L, N, k + 1, d, e2, &tau_s[(k + 1) & 1], vn);
             __syncthreads();
+            continue;
+        }
+        // partials of A22 v: thread (g, i) sums the columns j = g (mod G) of row i
+        const int G = min(16, TV_THREADS / m);
+        if (tid < G * m) {
+            const int i = tid % m, g = tid / m, I = s + i;
+            zc a0{0.0, 0.0}, a1{0.0, 0.0};  // two accumulators: shorter dependence chains
+            int j = g;
+            for (; j + G <= i; j += 2 * G) {  // row i of the lower part
+                cfma(a0, L[tv_col(s + j, N) + i - j], vk[j]);
+                cfma(a1, L[tv_col(s + j + G, N) + i - j - G], vk[j + G]);
+            }
+            if (j <= i) {
+                cfma(a0, L[tv_col(s + j, N) + i - j], vk[j]);
+                j += G;
+            }
+            const zc *ci = L + tv_col(I, N) - i;  // ci[j] = L(s + j, I), j > i
+            for (; j + G < m; j += 2 * G) {
+                cfma(a0, conj(ci[j]), vk[j]);
+                cfma(a1, conj(ci[j + G]), vk[j + G]);
+            }
+            if (j < m) cfma(a0, conj(ci[j]), vk[j]);
+            part[g * m + i] = a0 + a1;
+        }
+        __syncthreads();
+        // p = tau A22 v, the dot p^H v, w = p - (tau / 2)(p^H v) v
+        zc p{0.0, 0.0};
+        double dx = 0.0, dy = 0.0;
+        if (tid < m) {
+            zc acc = part[tid];
+            for (int g = 1; g < G; g++) acc = acc + part[g * m + tid];
+            p = t * acc;
+            const zc vi = vk[tid];
+            dx = p.x * vi.x + p.y * vi.y;
+            dy = p.x * vi.y - p.y * vi.x;
+        }
+        for (int o = 16; o; o >>= 1) {
+            dx += __shfl_xor_sync(FULL, dx, o);
+            dy += __shfl_xor_sync(FULL, dy, o);
+        }
+        if (lane == 0) {
+            red[warp][0] = dx;
+            red[warp][1] = dy;
+        }
+        __syncthreads();
+        if (tid < m) {
+            double rx[TV_WARPS], ry[TV_WARPS];  // pairwise sum of the warps' parts
 #pragma unroll
-            for (int u = 0; u < JV_TASKS; u++) {  // unrolled: task[] stays in registers
-                if (u >= ntask) break;
-                const int P1 = task[u] & 0xffff, P2 = task[u] >> 16;
-                const int p1 = sp[P1], q1 = sq[P1], p2 = sp[P2], q2 = sq[P2];
-                const bool r2 = q1 < N, c2 = q2 < N;
-                if (P1 == P2) {
-                    if (r2) {
-                        P[pk(p1, p1)] = zc{pa[P1], 0.0};
-                        P[pk(q1, q1)] = zc{pb[P1], 0.0};
-                        P[pk(p1, q1)] = zc{0.0, 0.0};
-                    }
-                    continue;
-                }
-                zc b00 = pget(P, p1, p2), b01{0.0, 0.0}, b10{0.0, 0.0}, b11{0.0, 0.0};
-                if (c2) b01 = pget(P, p1, q2);
-                if (r2) b10 = pget(P, q1, p2);
-                if (r2 && c2) b11 = pget(P, q1, q2);
-                if (r2) {  // rows: p <- c p - s ph q,  q <- s conj(ph) p + c q
-                    const double c = pc[P1], sv = ps[P1];
-                    const zc ph = pph[P1], wm = zc{-sv * ph.x, -sv * ph.y}, wp = zc{sv * ph.x, -sv * ph.y};
-                    zc x0 = c * b00, y0 = c * b10, x1 = c * b01, y1 = c * b11;
-                    cfma(x0, wm, b10);
-                    cfma(y0, wp, b00);
-                    cfma(x1, wm, b11);
-                    cfma(y1, wp, b01);
-                    b00 = x0;
-                    b10 = y0;
-                    b01 = x1;
-                    b11 = y1;
-                }
-                if (c2) {  // columns: p' <- c' p' - s' conj(ph') q',  q' <- s' ph' p' + c' q'
-                    const double c = pc[P2], sv = ps[P2];
-                    const zc ph = pph[P2], wm = zc{-sv * ph.x, sv * ph.y}, wp = zc{sv * ph.x, sv * ph.y};
-                    zc u0 = c * b00, v0 = c * b01, u1 = c * b10, v1 = c * b11;
-                    cfma(u0, wm, b01);
-                    cfma(v0, wp, b00);
-                    cfma(u1, wm, b11);
-                    cfma(v1, wp, b10);
-                    b00 = u0;
-                    b01 = v0;
-                    b10 = u1;
-                    b11 = v1;
-                }
-                pset(P, p1, p2, b00);
-                if (c2) pset(P, p1, q2, b01);
-                if (r2) pset(P, q1, p2, b10);
-                if (r2 && c2) pset(P, q1, q2, b11);
+            for (int q = 0; q < TV_WARPS; q++) {
+                rx[q] = red[q][0];
+                ry[q] = red[q][1];
             }
-            __syncthreads();
+#pragma unroll
+            for (int h = TV_WARPS / 2; h; h >>= 1)
+#pragma unroll
+                for (int q = 0; q < h; q++) {
+                    rx[q] += rx[q + h];
+                    ry[q] += ry[q + h];
+                }
+            const zc aw{-0.5 * (t.x * rx[0] - t.y * ry[0]), -0.5 * (t.x * ry[0] + t.y * rx[0])};
+            w[tid] = p + aw * vk[tid];
+        }
+        __syncthreads();
+        // A22 -= v w^H + w v^H on the lower triangle, one warp per column, the diagonal kept real;
+        // warp 0 updates column k + 1 alone and forms its reflector, warps 1.. the other columns
+        for (int j = warp; j < m; j += (warp == 0 ? m : TV_WARPS - 1)) {
+            zc *cj = L + tv_col(s + j, N) - j;  // cj[i] = L(s + i, s + j), i >= j
+            const zc vj = conj(vk[j]), wj = conj(w[j]);
+#pragma unroll 2
+            for (int i = j + lane; i < m; i += 32) {
+                zc x = cj[i] - vk[i] * wj - w[i] * vj;
+                if (i == j) x.y = 0.0;
+                cj[i] = x;
+            }
+            if (j == 0 && next) {  // column k + 1 is final: its reflector
+                __syncwarp();
+                tv_reflector(L, N, k + 1, d, e2, &tau_s[(k + 1) & 1], vn);
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) d[N - 1] = L[tv_col(N - 1, N)].x;
+    __syncthreads();
+    // phase 2: Gershgorin interval, pivmin (dstebz: the underflow threshold x max(1, max e^2))
+    if (warp == 0) {
+        double lo = INFINITY, hi = -INFINITY, me = 0.0;
+        for (int i = lane; i < N; i += 32) {
+            const double r = (i > 0 ? sqrt(e2[i - 1]) : 0.0) + (i + 1 < N ? sqrt(e2[i]) : 0.0);
+            lo = fmin(lo, d[i] - r);
+            hi = fmax(hi, d[i] + r);
+            if (i + 1 < N) me = fmax(me, e2[i]);
+        }
+        for (int o = 16; o; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(FULL, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(FULL, hi, o));
+            me = fmax(me, __shfl_xor_sync(FULL, me, o));
+        }
+        if (lane == 0) {
+            const double eps = 2.220446049250313e-16, tn = fmax(fabs(lo), fabs(hi));
+            const double pv = 2.2250738585072014e-308 * fmax(1.0, me);
+            const double widen = 2.0 * N * eps * tn + 2.0 * pv;
+            glo_s = lo - widen;
+            ghi_s = hi + widen;
+            piv_s = pv;
+            tol_s = 2.0 * eps * tn + 4.0 * pv;
         }
     }
-    // eigenvalues ascending (the order of jac_sort)
-    for (int i = tid; i < N; i += blockDim.x) dk[i] = P[pk(i, i)].x;
     __syncthreads();
-    for (int i = tid; i < N; i += blockDim.x) {
-        const double di = dk[i];
-        const bool ni = isnan(di);
-        const double ki = ni ? INFINITY : di;
-        int k = 0;
-        for (int j = 0; j < N; j++) {
-            const double dj = dk[j];
-            const bool nj = isnan(dj);
-            const double kj = nj ? INFINITY : dj;
-            k += kj < ki || (kj == ki && (nj < ni || (nj == ni && j < i)));
+    const double glo = glo_s, ghi = ghi_s, pv = piv_s, tol = tol_s;
+    // one count per thread at 512 points of the Gershgorin interval brackets every eigenvalue;
+    // then G threads per eigenvalue (32 / G eigenvalues per warp) split its bracket into G + 1
+    // parts per step
+    int *cnt = (int *)part;
+    const double step0 = (ghi - glo) / (TV_THREADS + 1);
+    cnt[tid] = tv_count(d, e2, N, glo + step0 * (tid + 1));
+    __syncthreads();
+    int G = 32;
+    while (G > 1 && TV_WARPS * (32 / G) < N) G--;
+    const int per = 32 / G, slot = lane / G, r = lane % G;
+    const int kk = warp * per + slot;
+    const bool own = slot < per && kk < N;
+    const int k = own ? kk : N - 1;
+    double lo = glo, hi = ghi;
+    for (int q = 0; q < TV_THREADS; q++) {
+        const double sq = glo + step0 * (q + 1);
+        if (cnt[q] <= k) lo = fmax(lo, sq);
+        else hi = fmin(hi, sq);
+    }
+    // the same number of steps for every group (the shuffles need all lanes)
+    int iters = 0;
+    for (double wd = step0; wd > tol && iters < 80; wd /= (G + 1)) iters++;
+    const int base = min(slot * G, 32 - G);
+    for (int it = 0; it < iters; it++) {
+        const double sg = lo + (hi - lo) * (double)(r + 1) / (double)(G + 1);
+        const int c = tv_count(d, e2, N, sg);
+        double nlo = lo, nhi = hi;
+        for (int q = 0; q < G; q++) {
+            const double sq = __shfl_sync(FULL, sg, base + q);
+            const int cq = __shfl_sync(FULL, c, base + q);
+            if (cq <= k) nlo = fmax(nlo, sq);
+            else nhi = fmin(nhi, sq);
         }
-        E[(int64_t)b * N + k] = ldexp(di, ex_s);
+        lo = nlo;
+        hi = nhi;
+    }
+    if (own && r == 0) {
+        // an isolated diagonal entry within the tolerance is the eigenvalue itself (the pivmin
+        // guard counts s = d_i as above d_i, so the bracket may end a pivmin short of it)
+        const double mid = 0.5 * (lo + hi);
+        double lam = mid, best = tol;
+        for (int i = 0; i < N; i++)
+            if ((i == 0 || e2[i - 1] == 0.0) && (i + 1 == N || e2[i] == 0.0) && fabs(d[i] - mid) <= best) {
+                best = fabs(d[i] - mid);
+                lam = d[i];
+            }
+        ev[k] = lam;
+    }
+    __syncthreads();
+    // ascending order (brackets of nearly equal eigenvalues may overlap)
+    for (int i = tid; i < N; i += TV_THREADS) {
+        const double x = ev[i];
+        int rank = 0;
+        for (int j = 0; j < N; j++) rank += ev[j] < x || (ev[j] == x && j < i);
+        E[(int64_t)b * N + rank] = ldexp(x, ex_s);
     }
 }
 
@@ -804,15 +922,15 @@ int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *
     std::vector<int> hinfo(batch, 0);
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return -(int)e;
-    const bool small = N <= JV_MAX_N;
+    const bool small = N <= TV_MAX_N;
     if ((e = setup_alloc((void **)&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
         (small || (e = setup_alloc((void **)&dW, sizeof(zc) * nn, st)) == cudaSuccess) &&
         (e = setup_alloc((void **)&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
         (e = setup_alloc((void **)&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
         (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess) {
         if (small) {
-            if ((e = smem_cap((const void *)jac_values)) == cudaSuccess) {
-                jac_values<<<batch, JV_THREADS, jv_smem(N), st>>>(N, dA, dE, dinfo);
+            if ((e = smem_cap((const void *)tri_values)) == cudaSuccess) {
+                tri_values<<<batch, TV_THREADS, tv_smem(N), st>>>(N, dA, dE, dinfo);
                 count_launch();
                 e = cudaGetLastError();
             }
