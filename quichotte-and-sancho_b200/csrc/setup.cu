@@ -28,8 +28,10 @@
 // first scaled by an exact power of two (jac_scale), so the sums of squares stay in range.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "qs_common.cuh"
@@ -823,6 +825,46 @@ __global__ void lowdin_scale(int N, const double *__restrict__ ev, zc *__restric
     }
 }
 
+// S^-1/2 for N <= 160 without eigenvectors: the coupled Newton-Schulz iteration (Higham,
+// Functions of Matrices, 2008, sec. 6.7) on A = S / ev_max, whose eigenvalues lie in (0, 1]:
+//   T = (3 I - Z Y) / 2,  Y <- Y T,  Z <- T Z,   Y0 = A, Z0 = I,   Z -> A^-1/2,
+// so S^-1/2 = Z / sqrt(ev_max), the same matrix function that U diag(ev^-1/2) U^T forms in the
+// reference (src/hamiltonian.f90:627-640). Every iterate is a polynomial in A, so each
+// eigenvalue follows the scalar map and the smallest one converges last: the host runs that
+// scalar map for ev_min / ev_max to fix the number of steps.
+__global__ void ns_init(int N, double c, const zc *__restrict__ S, zc *__restrict__ Y, zc *__restrict__ Z) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N * N; t += gridDim.x * blockDim.x) {
+        Y[t] = c * S[t];
+        Z[t] = zc{(t % N == t / N) ? 1.0 : 0.0, 0.0};
+    }
+}
+__global__ void ns_shift(int N, zc *__restrict__ T) {  // T <- (3 I - T) / 2
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N * N; t += gridDim.x * blockDim.x)
+        T[t] = zc{(t % N == t / N ? 1.5 : 0.0) - 0.5 * T[t].x, -0.5 * T[t].y};
+}
+// Smh = f (Z + Z^T) / 2, real (S is real); one thread per pair i <= j, so Smh may be Z
+__global__ void ns_final(int N, double f, const zc *Z, zc *Smh) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N * N; t += gridDim.x * blockDim.x) {
+        const int i = t % N, j = t / N;
+        if (i > j) continue;
+        const double v = 0.5 * f * (Z[i + (int64_t)j * N].x + Z[j + (int64_t)i * N].x);
+        Smh[i + (int64_t)j * N] = zc{v, 0.0};
+        Smh[j + (int64_t)i * N] = zc{v, 0.0};
+    }
+}
+static int ns_steps(double r) {  // r = ev_min / ev_max in (0, 1]
+    double y = r, z = 1.0;
+    int k = 0;
+    while (k < 200) {
+        const double t = 0.5 * (3.0 - z * y);
+        y *= t;
+        z *= t;
+        k++;
+        if (std::fabs(z * y - 1.0) <= 4e-16) break;
+    }
+    return k + 1;  // one more step: the error squares
+}
+
 // X2(2i+s, 2j+s) = X(i,j) (spin doubling, spin fastest; src/hamiltonian.f90:672-680)
 __global__ void spin_double(int N, const zc *__restrict__ X, zc *__restrict__ X2) {
     const int No = 2 * N;
@@ -909,11 +951,46 @@ int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, 
     return bad ? 1 : 0;
 }
 
+// N <= 160: one buffer [A | E | info], one launch of tri_values and one copy back, on the
+// calling thread's stream (the program calls this once, for the energy grid)
+static int eigenvalues_small(int N, int batch, const double *A, double *E, int *info) {
+    cudaStream_t st = cudaStreamPerThread;
+    const size_t bA = sizeof(zc) * (size_t)N * N * batch, bE = sizeof(double) * (size_t)N * batch;
+    const size_t bI = sizeof(int) * (size_t)batch;
+    std::vector<unsigned char> back(bE + bI);
+    unsigned char *buf = nullptr;
+    cudaError_t e = setup_alloc((void **)&buf, bA + bE + bI, st);
+    if (e != cudaSuccess) return -(int)e;
+    if ((e = cudaMemcpyAsync(buf, A, bA, cudaMemcpyHostToDevice, st)) == cudaSuccess &&
+        (e = smem_cap((const void *)tri_values)) == cudaSuccess) {
+        tri_values<<<batch, TV_THREADS, tv_smem(N), st>>>(N, (const zc *)buf, (double *)(buf + bA), (int *)(buf + bA + bE));
+        count_launch();
+        if ((e = cudaGetLastError()) == cudaSuccess &&
+            (e = cudaMemcpyAsync(back.data(), buf + bA, bE + bI, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+    }
+    cudaFreeAsync(buf, st);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        return -(int)e;
+    }
+    std::memcpy(E, back.data(), bE);
+    int bad = 0;
+    for (int b = 0; b < batch; b++) {
+        int v;
+        std::memcpy(&v, back.data() + bE + sizeof(int) * b, sizeof(int));
+        if (info) info[b] = v;
+        bad |= v;
+    }
+    return bad ? 1 : 0;
+}
+
 int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *info, int device) {
     if (N < 1 || N > JAC_MAX_N || batch < 0 || batch > 65535 || (batch > 0 && (!A || !E))) return -1;
     if (batch == 0) return 0;
     DeviceScope ds(device);
     if (ds.err != cudaSuccess) return -(int)ds.err;
+    if (N <= TV_MAX_N) return eigenvalues_small(N, batch, A, E, info);
     const size_t nn = (size_t)N * N * batch;
     cudaStream_t st = nullptr;
     zc *dA = nullptr, *dW = nullptr;
@@ -922,21 +999,12 @@ int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *
     std::vector<int> hinfo(batch, 0);
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return -(int)e;
-    const bool small = N <= TV_MAX_N;
     if ((e = setup_alloc((void **)&dA, sizeof(zc) * nn, st)) == cudaSuccess &&
-        (small || (e = setup_alloc((void **)&dW, sizeof(zc) * nn, st)) == cudaSuccess) &&
+        (e = setup_alloc((void **)&dW, sizeof(zc) * nn, st)) == cudaSuccess &&
         (e = setup_alloc((void **)&dE, sizeof(double) * (size_t)N * batch, st)) == cudaSuccess &&
         (e = setup_alloc((void **)&dinfo, sizeof(int) * batch, st)) == cudaSuccess &&
         (e = cudaMemcpyAsync(dA, A, sizeof(zc) * nn, cudaMemcpyHostToDevice, st)) == cudaSuccess) {
-        if (small) {
-            if ((e = smem_cap((const void *)tri_values)) == cudaSuccess) {
-                tri_values<<<batch, TV_THREADS, tv_smem(N), st>>>(N, dA, dE, dinfo);
-                count_launch();
-                e = cudaGetLastError();
-            }
-        } else {
-            e = eigh_dev(st, N, batch, dA, dE, dinfo, dW);  // the eigenvectors are not used
-        }
+        e = eigh_dev(st, N, batch, dA, dE, dinfo, dW);  // the eigenvectors are not used
         if (e == cudaSuccess &&
             (e = cudaMemcpyAsync(E, dE, sizeof(double) * (size_t)N * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess &&
             (e = cudaMemcpyAsync(hinfo.data(), dinfo, sizeof(int) * batch, cudaMemcpyDeviceToHost, st)) == cudaSuccess)
@@ -989,10 +1057,20 @@ int qs_dftb_lowdin(int N, const double *S, const double *H0, const double *Lam, 
         LOW_TRY(cudaMemcpyAsync(dR, S, sizeof(double) * n1, cudaMemcpyHostToDevice, st));
         LOW_TRY(cudaMemcpyAsync(dR + n1, H0, sizeof(double) * n1, cudaMemcpyHostToDevice, st));
         LOW_TRY(cudaMemcpyAsync(dLam, Lam, sizeof(zc) * n2, cudaMemcpyHostToDevice, st));
-        // S^-1/2 = U diag(ev^-1/2) U^T (src/hamiltonian.f90:627-640)
+        // S^-1/2 = U diag(ev^-1/2) U^T (src/hamiltonian.f90:627-640): for N <= 160 the
+        // eigenvalues by tri_values and the matrix function by Newton-Schulz, above by the
+        // Jacobi eigenpairs
+        const bool small = N <= TV_MAX_N;
         real_to_complex<<<gb, 256, 0, st>>>((int64_t)n1, dR, dS);
         count_launch();
-        LOW_TRY(eigh_dev(st, N, 1, dS, dE, dinfo, dW));
+        if (small) {
+            LOW_TRY(smem_cap((const void *)tri_values));
+            tri_values<<<1, TV_THREADS, tv_smem(N), st>>>(N, dS, dE, dinfo);
+            count_launch();
+            LOW_TRY(cudaGetLastError());
+        } else {
+            LOW_TRY(eigh_dev(st, N, 1, dS, dE, dinfo, dW));
+        }
         LOW_TRY(cudaMemcpyAsync(ev.data(), dE, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
         LOW_TRY(cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
         LOW_TRY(cudaStreamSynchronize(st));
@@ -1003,9 +1081,30 @@ int qs_dftb_lowdin(int N, const double *S, const double *H0, const double *Lam, 
             rc = 1;
             goto out;
         }
-        lowdin_scale<<<gb, 256, 0, st>>>(N, dE, dS);
-        count_launch();
-        zgemm(st, N, N, N, dS, N, dS, N, true, dSmh, N, 1.0, 0.0);  // W W^T, W real
+        if (small) {
+            double mx = ev[0];
+            for (int k = 1; k < N; k++) mx = std::fmax(mx, ev[k]);
+            const int steps = ns_steps(mn / mx);
+            // Y, Z and their successors, T: work blocks not yet in use (Hn, T, Hao, W)
+            zc *Y = dHn, *Yn = dT, *Z = dSmh, *Zn = dHao, *Tm = dW;
+            ns_init<<<gb, 256, 0, st>>>(N, 1.0 / mx, dS, Y, Z);
+            count_launch();
+            for (int q = 0; q < steps; q++) {
+                zgemm(st, N, N, N, Z, N, Y, N, false, Tm, N, 1.0, 0.0);
+                ns_shift<<<gb, 256, 0, st>>>(N, Tm);
+                count_launch();
+                zgemm(st, N, N, N, Y, N, Tm, N, false, Yn, N, 1.0, 0.0);
+                zgemm(st, N, N, N, Tm, N, Z, N, false, Zn, N, 1.0, 0.0);
+                std::swap(Y, Yn);
+                std::swap(Z, Zn);
+            }
+            ns_final<<<gb, 256, 0, st>>>(N, 1.0 / std::sqrt(mx), Z, dSmh);
+            count_launch();
+        } else {
+            lowdin_scale<<<gb, 256, 0, st>>>(N, dE, dS);
+            count_launch();
+            zgemm(st, N, N, N, dS, N, dS, N, true, dSmh, N, 1.0, 0.0);  // W W^T, W real
+        }
         spin_double<<<gb, 256, 0, st>>>(N, dSmh, dSm2);
         count_launch();
         // Hao = H0 spin-doubled, plus the SOC form (src/hamiltonian.f90:670-687)

@@ -104,12 +104,15 @@ def _lowdin_numpy(S, H0, Lam, dual):
     return 0.5 * (H + H.conj().T), ev.min()
 
 
-@pytest.mark.parametrize("N,dual", [(1, True), (9, True), (31, False), (124, True)])
-def test_dftb_lowdin_matches_numpy(N, dual):
+# N <= 160: S^-1/2 by Newton-Schulz on the eigenvalues of one block; above: the Jacobi eigenpairs.
+# spread = ||S - I||_2 (0.99: condition number ~200, 13 Newton-Schulz steps; 0: S = I)
+@pytest.mark.parametrize("N,dual,spread", [(1, True, 0.1), (9, True, 0.1), (31, False, 0.1), (124, True, 0.1),
+                                           (80, True, 0.99), (5, False, 0.0), (200, True, 0.1)])
+def test_dftb_lowdin_matches_numpy(N, dual, spread):
     rng = np.random.default_rng(7 + N)
     P = rng.standard_normal((N, N))
     P = 0.5 * (P + P.T)
-    S = np.eye(N) + 0.1 * P / max(1.0, np.linalg.norm(P, 2))
+    S = np.eye(N) + spread * P / max(1e-300, np.linalg.norm(P, 2))
     H0 = rng.standard_normal((N, N))
     H0 = 0.5 * (H0 + H0.T) * 27.211386245988
     Lam = 0.01 * _herm(rng, 2 * N)
