@@ -130,16 +130,19 @@ int qs_invert_batched(int N, int batch, double *A, int *info, int precision);
 int qs_hermitian_eigensystem(int N, int batch, double *A, double *E, int *info, int device);
 
 /* The same eigenvalues without the eigenvectors (zheev with JOBZ = 'N'), as the energy grid
- * needs them (src/quichotte.f90:81-83): A is not modified. For N <= 160 each matrix is
- * diagonalised by one thread block with the matrix in shared memory (one launch for the
- * batch); larger N takes the path of qs_hermitian_eigensystem. Same info, limits and
- * returns. */
+ * needs them (src/quichotte.f90:81-83): A is not modified. For N <= 160 one thread block per
+ * matrix, with the matrix in shared memory, reduces it to a real tridiagonal matrix by
+ * Householder reflectors and finds the eigenvalues by Sturm-count multisection (one launch
+ * for the batch; info[b] = 1 only for non-finite entries); larger N takes the path of
+ * qs_hermitian_eigensystem. Same info, limits and returns. */
 int qs_hermitian_eigenvalues(int N, int batch, const double *A, double *E, int *info, int device);
 
 /* The dense linear algebra of build_hamiltonian_from_dftb_hs (src/hamiltonian.f90:625-689):
  * S (N x N real symmetric overlap) and H0 (N x N real, eV) as the reference holds them after
  * symmetrisation, Lam (2N x 2N complex, the p-shell SOC matrix, spin fastest);
- *   S^-1/2 = U diag(s^-1/2) U^T from the eigenpairs of S,
+ *   S^-1/2 = U diag(s^-1/2) U^T (for N > 160 from the eigenpairs of S; for N <= 160 the same
+ *            matrix function by the coupled Newton-Schulz iteration, the step count fixed by
+ *            the eigenvalues of S),
  *   Hao = H0 (x) I2 + (soc_dual ? (Sx2 Lam + Lam Sx2)/2 : Lam),   Sx2 = S (x) I2,
  *   H = (Sm2 Hao Sm2 + its conjugate transpose)/2,                 Sm2 = S^-1/2 (x) I2,
  * into H (2N x 2N complex). evmin receives the smallest eigenvalue of S. Returns 0, 1 if S is
