@@ -687,7 +687,10 @@ def setup_timing(qb, m, repeats=3):
     E, _, info = qb.hermitian_eigensystem(m.H)
     Hd, _ = qb.dftb_lowdin(S, H0, Lam, True)
     Hn = lowdin_numpy()
+    Ev, _ = qb.hermitian_eigenvalues(m.H)
     return {"eigenvalues_ms": best(lambda: qb.hermitian_eigenvalues(m.H)),
+            "eigenvalues_numpy_ms": best(lambda: np.linalg.eigvalsh(m.H)),
+            "eigenvalues_rel_err": float(np.max(np.abs(Ev - np.linalg.eigvalsh(m.H))) / np.max(np.abs(Ev))),
             "eigensystem_ms": best(lambda: qb.hermitian_eigensystem(m.H)),
             "eigensystem_numpy_ms": best(lambda: np.linalg.eigh(m.H)),
             "eigensystem_rel_err": float(np.max(np.abs(E - np.linalg.eigvalsh(m.H))) / np.max(np.abs(E))),
